@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Throughput of the B200 template-matching path on the Neuropixels-scale workload.
+
+Workload: C=384 channels (Neuropixels-1.0-like geometry), K=600 templates,
+20 batches of 60000 samples (+2*61 padding), nt=61, n_pcs=6, Th_learned=8,
+seeded synthetic data (kilosort_b200.synth, seed 1002).  A step is one pass of
+`run_matching` over all 20 batches with X resident in HBM (1.85 GB per step,
+larger than L2).  `value` is channel-samples/s of the split-BF16 projection
+form; the plain-FP32 form is timed in the same run.  `e2e` runs the same
+workload through the public `run_matching` from pinned host memory, with the
+host->device copy of X and the device->host copy of the spikes inside the
+timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --impl reference rank 0 times the CPU oracle of the reference's
+run_matching (torch on all host threads) on a bounded sample of the same
+workload (one batch per step).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+NT_BATCH = 60000
+NT = 61
+N_PCS = 6
+TH = 8.0
+CFG = 2
+WORKLOAD = ("Neuropixels-scale matching: C=384 (NP1-like), K=600 templates, 20 batches x "
+            "60000 samples (+2*61 pad), nt=61, n_pcs=6, Th_learned=8, max_peels=100")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--batches", type=int, default=20)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_batch(rec, b, threads):
+    from oracle import matching as om
+    torch.set_num_threads(threads)
+    U = torch.from_numpy(rec.U)
+    W = torch.from_numpy(rec.wPCA)
+    ops = dict(Th_learned=TH, nt=NT, max_peels=100, wPCA=W)
+    ctc = om.prepare_matching(ops, U)
+    X = torch.from_numpy(np.ascontiguousarray(rec.batch(b)))
+    t0 = time.perf_counter()
+    st, amps, th, _ = om.run_matching(ops, X, U, ctc)
+    dt = time.perf_counter() - t0
+    return st.numpy(), amps.numpy(), dt
+
+
+def reference_arm(args, rank):
+    """CPU oracle of the reference's run_matching, one cfg-2 batch per step."""
+    if rank != 0:
+        return
+    from kilosort_b200 import synth
+    threads = os.cpu_count() or 1
+    rec = synth.config_recording(CFG, n_batches=1)
+    times = []
+    for i in range(args.warmup + args.steps):
+        _, _, dt = cpu_oracle_batch(rec, 0, threads)
+        if i >= args.warmup:
+            times.append(dt)
+    t = statistics.median(times)
+    v = rec.n_chan * NT_BATCH / t
+    line = {
+        "impl": "reference", "metric": "channel-samples/s", "value": v,
+        "unit": "channel-samples/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": "batch 0 of the 20 per step"},
+        "cpu_baseline": {"value": v, "unit": "channel-samples/s", "cores": threads,
+                         "kind": "port", "sample": "1 batch (C=384, 60000 samples) per step"},
+        "e2e": {"value": v, "unit": "channel-samples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    import datetime
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    import kilosort_b200 as kb
+    from kilosort_b200 import _lib, synth
+    from tests.parity_util import agreement
+
+    rec = synth.config_recording(CFG, n_batches=args.batches)
+    C, K = rec.n_chan, rec.n_templates
+    L = NT_BATCH + 2 * NT
+    U = torch.from_numpy(rec.U).to(dev)
+    W = torch.from_numpy(rec.wPCA).to(dev)
+    Xs = [torch.from_numpy(np.ascontiguousarray(rec.batch(b))).to(dev) for b in range(args.batches)]
+    Xh = [torch.from_numpy(np.ascontiguousarray(rec.batch(b))).pin_memory() for b in range(args.batches)]
+    ops = dict(Th_learned=TH, nt=NT, max_peels=100, wPCA=W)
+    ctc = kb.prepare_matching(ops, U)
+    torch.cuda.synchronize()
+
+    # projection forms available in this build
+    forms = ["fp32"]
+    try:
+        kb.run_matching(dict(ops, projection="bf16x3"), Xs[0], U, ctc, device=dev)
+        forms.append("bf16x3")
+    except _lib.KilosortB200Error as e:
+        if e.status != _lib.KS_ERR_UNSUPPORTED:
+            raise
+    head = forms[-1]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    def device_step(form, spikes):
+        o = dict(ops, projection=form)
+        n = 0
+        for X in Xs:
+            st, _, _, _ = kb.run_matching(o, X, U, ctc, device=dev)
+            n += len(st)
+        spikes.append(n)
+
+    def timed(fn, form, sampler=None):
+        for _ in range(args.warmup):
+            fn(form, [])
+        barrier()
+        spikes = []
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if sampler:
+            sampler.__enter__()
+        s0.record()
+        for _ in range(args.steps):
+            fn(form, spikes)
+        s1.record()
+        barrier()
+        if sampler:
+            sampler.__exit__()
+        ms = max_over_ranks(s0.elapsed_time(s1)) / args.steps
+        return ms, spikes[-1]
+
+    sampler = ClockSampler(local)
+    results = {}
+    for form in forms:
+        ms, nsp = timed(device_step, form, sampler if form == head else None)
+        results[form] = dict(ms=ms, spikes=nsp)
+
+    # end to end from pinned host memory through the public API
+    h2d = C * L * 4 * args.batches
+    d2h = [0]
+
+    def e2e_step(form, spikes):
+        o = dict(ops, projection=form)
+        n = 0
+        d2h[0] = 0
+        for Xhost in Xh:
+            X = Xhost.to(dev, non_blocking=True)
+            st, amps, th, _ = kb.run_matching(o, X, U, ctc, device=dev)
+            st_h, a_h, t_h = st.cpu(), amps.cpu(), th.cpu()
+            n += len(st_h)
+            d2h[0] += st_h.numel() * 8 + a_h.numel() * 4 + t_h.numel() * 4
+        spikes.append(n)
+
+    e2e_ms, _ = timed(e2e_step, head)
+
+    # stage breakdown of one pass (projection vs peel) for the roofline
+    stage = {"project": 0.0, "peel": 0.0}
+    kused, nsp_total = 0, 0
+    ldb = ((L + 63) // 64) * 64
+    Bbuf = torch.empty((K, ldb), dtype=torch.float32, device=dev)
+    nm = kb.template_energy(U)
+    for X in Xs:
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        B = kb.project_scores(X, U, W, NT, head)
+        e[1].record()
+        Bbuf[:, :L].copy_(B)
+        Xres = X.clone()
+        e2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        e2[0].record()
+        st, amps, th, _ = kb.peel(Bbuf[:, :L], Xres, U, W, ctc, nm, TH, NT, 100)
+        e2[1].record()
+        torch.cuda.synchronize()
+        stage["project"] += e[0].elapsed_time(e[1])
+        stage["peel"] += e2[0].elapsed_time(e2[1])
+        kused += len(torch.unique(st[:, 1]))
+        nsp_total += len(st)
+    nb = args.batches
+    hbm, bf16, peak_kind = peaks()
+    flop_proj = 2.0 * L * C * N_PCS * (NT + K) * nb
+    bytes_peel = (4.0 * K * L + 8.0 * C * L) * nb + 4.0 * K * (2 * NT + 1) * kused \
+        + 4.0 * N_PCS * C * kused + 24.0 * nsp_total
+    proj_tflops = flop_proj / (stage["project"] * 1e-3) / 1e12
+    peel_gbs = bytes_peel / (stage["peel"] * 1e-3) / 1e9
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    if stage["peel"] >= stage["project"]:
+        roof = {"kernel": "peel", "bound": "hbm", "achieved": peel_gbs, "peak": hbm,
+                "unit": "GB/s", "frac": peel_gbs / hbm, "traffic": None,
+                "peak_source": peak_kind}
+    elif head == "bf16x3":
+        roof = {"kernel": "project_bf16x3", "bound": "tensor", "achieved": proj_tflops,
+                "peak": bf16, "unit": "TFLOP/s", "frac": proj_tflops / bf16, "traffic": None,
+                "peak_source": peak_kind}
+    else:
+        roof = {"kernel": "project_fp32", "bound": "fp32-simt", "achieved": proj_tflops,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": proj_tflops / fp32_peak,
+                "traffic": None, "peak_source": "nominal FP32 FMA"}
+
+    cpu = None
+    agr = {}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        st_r, amps_r, dt = cpu_oracle_batch(rec, 0, threads)
+        cpu = {"value": C * NT_BATCH / dt, "unit": "channel-samples/s", "cores": threads,
+               "kind": "port", "sample": "batch 0 (C=384, 60000 samples), oracle run_matching"}
+        for form in forms:
+            st, amps, _, _ = kb.run_matching(dict(ops, projection=form), Xs[0], U, ctc, device=dev)
+            a = agreement(st.cpu().numpy(), st_r, amps.cpu().numpy(), amps_r)
+            agr[form] = {k: a[k] for k in ("agreement", "amp_rel_max", "matched", "n_a", "n_r")}
+
+    launches_per_batch = 5  # energy, reorder, temporal, contraction, peel
+    per_step_samples = C * NT_BATCH * nb
+    head_ms = results[head]["ms"]
+    value = per_step_samples * world / (head_ms * 1e-3)
+    line = {
+        "metric": "channel-samples/s", "value": value, "unit": "channel-samples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": head_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if head == "fp32" else "f32 (split-bf16 projection)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "projection": head, "batches": nb,
+                   "l2": "inputs larger than L2 (1.85 GB of X per step)",
+                   "parallelism": f"replicas x{world}"},
+        "spikes_per_s": results[head]["spikes"] * world / (head_ms * 1e-3),
+        "forms": {f: {"ms_per_step": r["ms"],
+                      "channel_samples_per_s": per_step_samples * world / (r["ms"] * 1e-3),
+                      "spikes_per_step": r["spikes"]} for f, r in results.items()},
+        "speedup_split_vs_fp32": (results["fp32"]["ms"] / results["bf16x3"]["ms"]
+                                  if "bf16x3" in results else None),
+        "stages_ms_per_step": stage,
+        "agreement_vs_oracle_batch0": agr,
+        "e2e": {"value": per_step_samples * world / (e2e_ms * 1e-3), "unit": "channel-samples/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h[0],
+                "ms_per_step": e2e_ms},
+        "roofline": roof,
+        "roofline_all": {"project": {"achieved_tflops": proj_tflops},
+                         "peel": {"achieved_gbs": peel_gbs, "algorithmic_bytes": bytes_peel}},
+        "cpu_baseline": cpu,
+        "clocks": sampler.summary(),
+        "gpu_launches": launches_per_batch * nb,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,145 @@
+/*
+ * ks_b200.h -- C ABI of the B200-native Kilosort4 template-matching path.
+ *
+ * Every entry point takes raw device pointers (row-major, contiguous unless a
+ * leading dimension is given), int64 sizes, a CUDA stream (cudaStream_t passed
+ * as void*) and, where scratch is needed, a caller-owned device workspace whose
+ * size is returned by the matching *_workspace_size() query.  The library never
+ * allocates device memory and never synchronises the stream, except where a
+ * function says so.  Return value: 0 (KS_OK) or a KS_ERR_* code; a readable
+ * message for the last failure on the calling thread is in ks_last_error().
+ *
+ * Device-side outcomes of the greedy peel (spike count, iterations, overflow,
+ * watchdog) are written to a caller-provided int64 "info" array on the device:
+ *   info[0] = spikes written, info[1] = status (KS_OK or KS_ERR_*),
+ *   info[2] = iterations run, info[3] = spikes the batch needed (when it
+ *   overflowed the capacity).
+ *
+ * Shapes use the reference's names: C = n channels, L = padded batch length
+ * (NT + 2*nt), K = n templates, P = n_pcs, nt = template length (odd).
+ */
+#ifndef KS_B200_H
+#define KS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define KS_API __attribute__((visibility("default")))
+#else
+#define KS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define KS_OK 0
+#define KS_ERR_ARG 1          /* invalid argument (size, alignment, null) */
+#define KS_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define KS_ERR_OVERFLOW 3     /* more spikes than the output capacity */
+#define KS_ERR_TIMEOUT 4      /* a bounded device-side wait ran out */
+#define KS_ERR_WORKSPACE 5    /* workspace smaller than *_workspace_size() */
+#define KS_ERR_UNSUPPORTED 6  /* device or shape not supported by this build */
+#define KS_ERR_DEGENERATE 7   /* exact score plateaus beyond the tie buffer */
+
+/* projection precision */
+#define KS_PROJ_FP32 0        /* plain FP32 (SIMT) contraction */
+#define KS_PROJ_BF16X3 1      /* split-BF16 hi/lo, three tcgen05 MMAs, FP32 accumulate */
+
+KS_API int ks_version(void);
+KS_API const char* ks_status_string(int status);
+KS_API const char* ks_last_error(void);
+
+/*
+ * Template energy, nm[k] = sum_{p,c} U[k,p,c]^2.
+ * Replaces kilosort/template_matching.py:176.
+ */
+KS_API int ks_template_energy(const float* U, int64_t K, int64_t P, int64_t C,
+                       float* nm, void* stream);
+
+/*
+ * Score matrix B[k, tau] = sum_{p,c} U[k,p,c] * sum_t W[p,t] X[c, tau - nt/2 + t]
+ * (zero padding), written with leading dimension ldb >= L.
+ * Replaces kilosort/template_matching.py:180-181 (conv1d + einsum).
+ */
+KS_API size_t ks_project_workspace_size(int64_t C, int64_t L, int64_t K, int64_t P,
+                                 int precision);
+KS_API int ks_project(const float* X, const float* U, const float* W,
+               int64_t C, int64_t L, int64_t K, int64_t P, int64_t nt,
+               int precision, float* B, int64_t ldb,
+               void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Greedy peel on a score matrix (B [K, ldb], modified in place) and a residual
+ * (Xres [C, L], modified in place): up to max_peels iterations of detect /
+ * record / subtract.  Outputs st [capacity, 2] int64 (tau, template),
+ * amps [capacity], th_amps [capacity] float32, in the reference's order
+ * (iteration, then tau).  th2 = Th_learned^2 rounded to float32.
+ * Replaces kilosort/template_matching.py:183-244.
+ */
+KS_API size_t ks_peel_workspace_size(int64_t L, int64_t K);
+KS_API int ks_peel(float* B, int64_t ldb, float* Xres, const float* U, const float* W,
+            const float* ctc, const float* nm,
+            int64_t C, int64_t L, int64_t K, int64_t P, int64_t nt,
+            float th2, int64_t max_peels, int64_t capacity,
+            int64_t* st, float* amps, float* th_amps, int64_t* info,
+            void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Whole per-batch matching: Xres <- X, nm, scores, peel.
+ * Replaces kilosort/template_matching.py:170-244 (run_matching).
+ */
+KS_API size_t ks_run_matching_workspace_size(int64_t C, int64_t L, int64_t K,
+                                      int64_t P, int precision);
+KS_API int ks_run_matching(const float* X, const float* U, const float* W,
+                    const float* ctc, int64_t C, int64_t L, int64_t K,
+                    int64_t P, int64_t nt, float th2, int64_t max_peels,
+                    int precision, int64_t capacity,
+                    int64_t* st, float* amps, float* th_amps, float* Xres,
+                    int64_t* info, void* workspace, size_t workspace_bytes,
+                    void* stream);
+
+/*
+ * Per-spike PC features: tF[s, i, p] = sum_t Xres[iCC[i, iU[k_s]], tau_s - nt/2 + t]
+ * * W[p, t] + amps[s] * Ucc[i, k_s, p], for s < n_spikes (st/amps as written
+ * by ks_peel).  tF is [n_spikes, nC, P].
+ * Replaces kilosort/template_matching.py:85-86 (with the transpose at :108).
+ */
+KS_API int ks_features(const float* Xres, const int64_t* st, const float* amps,
+                const float* W, const int64_t* iCC, const int64_t* iU,
+                const float* Ucc, int64_t C, int64_t L, int64_t K, int64_t P,
+                int64_t nt, int64_t nC, int64_t n_spikes, float* tF,
+                void* stream);
+
+/*
+ * Per-template peak channel and feature loadings: iU[k] = argmax_c
+ * sum_p U[k,p,c]^2 (first index on ties), Ucc[i,k,p] = U[k,p,iCC[i,iU[k]]].
+ * Replaces the device part of kilosort/template_matching.py:50-51.
+ */
+KS_API int ks_template_channels(const float* U, const int64_t* iCC, int64_t K,
+                         int64_t P, int64_t C, int64_t nC, int64_t* iU,
+                         float* Ucc, void* stream);
+
+/*
+ * Template cross-correlations ctc [K, K, 2*nt+1].
+ * Replaces kilosort/template_matching.py:155-167 (prepare_matching).
+ */
+KS_API size_t ks_ctc_workspace_size(int64_t K, int64_t P, int64_t C, int64_t nt);
+KS_API int ks_ctc(const float* U, const float* W, int64_t K, int64_t P, int64_t C,
+           int64_t nt, float* ctc, void* workspace, size_t workspace_bytes,
+           void* stream);
+
+/*
+ * Watchdog self-test: one thread waits on a device flag that nothing sets,
+ * bounded by timeout_ns, and writes KS_ERR_TIMEOUT to status[0] when the wait
+ * runs out.  status points to two device ints (status[1] is the flag, cleared
+ * here).  No reference counterpart (tests the device-side bounded waits).
+ */
+KS_API int ks_selftest_wait(int64_t timeout_ns, int* status, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KS_B200_H */

@@ -1,0 +1,100 @@
+"""ctypes binding of ``libks_b200.so`` (the C ABI in ``include/ks_b200.h``).
+
+The library is built in-tree by ``python -m kilosort_b200.build``.  Loading it
+needs no GPU (the CUDA runtime is linked statically); calling any compute entry
+point needs a B200.  There is no fallback: if the library is missing, every
+compute call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libks_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "ks_b200.h")
+
+KS_OK = 0
+KS_ERR_ARG = 1
+KS_ERR_CUDA = 2
+KS_ERR_OVERFLOW = 3
+KS_ERR_TIMEOUT = 4
+KS_ERR_WORKSPACE = 5
+KS_ERR_UNSUPPORTED = 6
+KS_ERR_DEGENERATE = 7
+
+KS_PROJ_FP32 = 0
+KS_PROJ_BF16X3 = 1
+
+_i64, _f32, _int, _sz, _vp = C.c_int64, C.c_float, C.c_int, C.c_size_t, C.c_void_p
+
+# name -> (restype, argtypes); pointers are passed as integers (c_void_p)
+SIGNATURES = {
+    "ks_version": (_int, []),
+    "ks_status_string": (C.c_char_p, [_int]),
+    "ks_last_error": (C.c_char_p, []),
+    "ks_template_energy": (_int, [_vp, _i64, _i64, _i64, _vp, _vp]),
+    "ks_project_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _int]),
+    "ks_project": (_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _vp,
+                          _i64, _vp, _sz, _vp]),
+    "ks_peel_workspace_size": (_sz, [_i64, _i64]),
+    "ks_peel": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64,
+                       _i64, _f32, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "ks_run_matching_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _int]),
+    "ks_run_matching": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
+                               _f32, _i64, _int, _i64, _vp, _vp, _vp, _vp, _vp,
+                               _vp, _sz, _vp]),
+    "ks_features": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64,
+                           _i64, _i64, _i64, _i64, _vp, _vp]),
+    "ks_template_channels": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp]),
+    "ks_ctc_workspace_size": (_sz, [_i64, _i64, _i64, _i64]),
+    "ks_ctc": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp, _sz, _vp]),
+    "ks_selftest_wait": (_int, [_i64, _vp, _vp]),
+}
+
+_lib = None
+
+
+class KilosortB200Error(RuntimeError):
+    """A C-ABI call returned a nonzero status."""
+
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+def header_symbols():
+    """Names of the functions declared in include/ks_b200.h."""
+    with open(HEADER) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"KS_API\s+[\w\s\*]+?\b(ks_\w+)\s*\(", text)))
+
+
+def load():
+    """Load the shared library once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m kilosort_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status, what):
+    if status != KS_OK:
+        lib = load()
+        msg = lib.ks_last_error().decode(errors="replace")
+        name = lib.ks_status_string(status).decode()
+        raise KilosortB200Error(status, f"{what}: {name} ({status}): {msg}")
+
+
+def status_message(status):
+    return load().ks_status_string(int(status)).decode()

@@ -1,0 +1,238 @@
+// extern "C" entry points declared in include/ks_b200.h.
+#include "ks_common.cuh"
+#include "project.cuh"
+
+#include <algorithm>
+#include <cstdlib>
+#include <string>
+
+namespace ks {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+  set_error(msg);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return KS_ERR_CUDA;
+}
+
+int device_info(DeviceInfo* out) {
+  static thread_local DeviceInfo cache[64];
+  int dev = 0;
+  KS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(KS_ERR_UNSUPPORTED, "device index out of range");
+  DeviceInfo& d = cache[dev];
+  if (d.device != dev) {
+    cudaDeviceProp prop;
+    KS_CUDA(cudaGetDeviceProperties(&prop, dev));
+    d.sm_count = prop.multiProcessorCount;
+    d.cc_major = prop.major;
+    d.cc_minor = prop.minor;
+    d.smem_optin = prop.sharedMemPerBlockOptin;
+    d.device = dev;
+  }
+  if (d.cc_major != 10)
+    return fail(KS_ERR_UNSUPPORTED, "this library is built for sm_100a (B200) only");
+  *out = d;
+  return KS_OK;
+}
+
+static unsigned long long wait_limit_ns() {
+  static unsigned long long v = [] {
+    const char* s = std::getenv("KS_B200_WAIT_LIMIT_NS");
+    unsigned long long x = s ? std::strtoull(s, nullptr, 10) : 0ull;
+    return x ? x : kWaitLimitNs;
+  }();
+  return v;
+}
+
+size_t ctc_workspace_size(int64_t K, int64_t P, int64_t C, int64_t nt);
+int launch_ctc(const float* U, const float* W, int64_t K, int64_t P, int64_t C,
+               int64_t nt, float* ctc, void* ws, size_t ws_bytes, cudaStream_t stream);
+int launch_features(const float* Xres, const int64_t* st, const float* amps,
+                    const float* W, const int64_t* iCC, const int64_t* iU,
+                    const float* Ucc, int64_t C, int64_t L, int64_t K, int64_t P,
+                    int64_t nt, int64_t nC, int64_t N, float* tF, cudaStream_t stream);
+int launch_template_channels(const float* U, const int64_t* iCC, int64_t K,
+                             int64_t P, int64_t C, int64_t nC, int64_t* iU,
+                             float* Ucc, cudaStream_t stream);
+
+// Layout of the run_matching workspace: nm, B, projection scratch, peel scratch.
+struct MatchLayout {
+  int64_t ldb;
+  size_t nm_off, b_off, proj_off, peel_off, bytes;
+};
+
+static MatchLayout match_layout(int64_t C, int64_t L, int64_t K, int64_t P, int precision) {
+  MatchLayout m;
+  m.ldb = round_up(L, 64);
+  size_t off = 0;
+  m.nm_off = off;
+  off = align256(off + sizeof(float) * K);
+  m.b_off = off;
+  off = align256(off + sizeof(float) * (size_t)K * m.ldb);
+  m.proj_off = off;
+  off = align256(off + proj_layout(C, L, K, P, precision).bytes);
+  m.peel_off = off;
+  off = align256(off + peel_workspace_size(L));
+  m.bytes = off;
+  return m;
+}
+
+__global__ void ks_wait_never_kernel(unsigned long long limit_ns, int* status,
+                                     const int* flag) {
+  const unsigned long long t0 = ks_globaltimer();
+  int st = KS_OK;
+  while (ks_ld_volatile(flag) == 0) {
+    __nanosleep(1000);
+    if (ks_globaltimer() - t0 > limit_ns) {
+      st = KS_ERR_TIMEOUT;
+      break;
+    }
+  }
+  *status = st;
+}
+
+}  // namespace ks
+
+using namespace ks;
+
+extern "C" {
+
+int ks_version(void) { return 1; }
+
+const char* ks_status_string(int status) {
+  switch (status) {
+    case KS_OK: return "ok";
+    case KS_ERR_ARG: return "invalid argument";
+    case KS_ERR_CUDA: return "CUDA error";
+    case KS_ERR_OVERFLOW: return "spike buffer overflow";
+    case KS_ERR_TIMEOUT: return "device-side wait timed out";
+    case KS_ERR_WORKSPACE: return "workspace too small";
+    case KS_ERR_UNSUPPORTED: return "unsupported device or shape";
+    case KS_ERR_DEGENERATE: return "score plateau beyond the tie buffer";
+    default: return "unknown status";
+  }
+}
+
+const char* ks_last_error(void) { return g_last_error.c_str(); }
+
+int ks_template_energy(const float* U, int64_t K, int64_t P, int64_t C, float* nm,
+                       void* stream) {
+  return launch_template_energy(U, K, P, C, nm, static_cast<cudaStream_t>(stream));
+}
+
+size_t ks_project_workspace_size(int64_t C, int64_t L, int64_t K, int64_t P,
+                                 int precision) {
+  return proj_layout(C, L, K, P, precision).bytes;
+}
+
+int ks_project(const float* X, const float* U, const float* W, int64_t C,
+               int64_t L, int64_t K, int64_t P, int64_t nt, int precision,
+               float* B, int64_t ldb, void* workspace, size_t workspace_bytes,
+               void* stream) {
+  if (!X || !U || !W || !B) return fail(KS_ERR_ARG, "ks_project: null pointer");
+  DeviceInfo d;
+  int rc = device_info(&d);
+  if (rc) return rc;
+  return launch_project(X, U, W, C, L, K, P, nt, precision, B, ldb, workspace,
+                        workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+size_t ks_peel_workspace_size(int64_t L, int64_t K) {
+  (void)K;
+  return peel_workspace_size(L);
+}
+
+int ks_peel(float* B, int64_t ldb, float* Xres, const float* U, const float* W,
+            const float* ctc, const float* nm, int64_t C, int64_t L, int64_t K,
+            int64_t P, int64_t nt, float th2, int64_t max_peels, int64_t capacity,
+            int64_t* st, float* amps, float* th_amps, int64_t* info,
+            void* workspace, size_t workspace_bytes, void* stream) {
+  return launch_peel(B, ldb, Xres, U, W, ctc, nm, C, L, K, P, nt, th2, max_peels,
+                     capacity, st, amps, th_amps, info, workspace, workspace_bytes,
+                     static_cast<cudaStream_t>(stream), wait_limit_ns());
+}
+
+size_t ks_run_matching_workspace_size(int64_t C, int64_t L, int64_t K, int64_t P,
+                                      int precision) {
+  return match_layout(C, L, K, P, precision).bytes;
+}
+
+int ks_run_matching(const float* X, const float* U, const float* W,
+                    const float* ctc, int64_t C, int64_t L, int64_t K, int64_t P,
+                    int64_t nt, float th2, int64_t max_peels, int precision,
+                    int64_t capacity, int64_t* st, float* amps, float* th_amps,
+                    float* Xres, int64_t* info, void* workspace,
+                    size_t workspace_bytes, void* stream) {
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!X || !Xres) return fail(KS_ERR_ARG, "ks_run_matching: null pointer");
+  if (C < 1 || L < 1 || K < 1 || P < 1) return fail(KS_ERR_ARG, "ks_run_matching: bad sizes");
+  if (precision != KS_PROJ_FP32 && precision != KS_PROJ_BF16X3)
+    return fail(KS_ERR_ARG, "ks_run_matching: unknown precision");
+  const MatchLayout m = match_layout(C, L, K, P, precision);
+  if (!workspace || workspace_bytes < m.bytes)
+    return fail(KS_ERR_WORKSPACE, "ks_run_matching: workspace too small");
+  DeviceInfo d;
+  int rc = device_info(&d);
+  if (rc) return rc;
+  char* base = static_cast<char*>(workspace);
+  float* nm = reinterpret_cast<float*>(base + m.nm_off);
+  float* B = reinterpret_cast<float*>(base + m.b_off);
+  if (Xres != X)
+    KS_CUDA(cudaMemcpyAsync(Xres, X, sizeof(float) * C * L, cudaMemcpyDeviceToDevice, s));
+  rc = launch_template_energy(U, K, P, C, nm, s);
+  if (rc) return rc;
+  rc = launch_project(X, U, W, C, L, K, P, nt, precision, B, m.ldb, base + m.proj_off,
+                      m.peel_off - m.proj_off, s);
+  if (rc) return rc;
+  return launch_peel(B, m.ldb, Xres, U, W, ctc, nm, C, L, K, P, nt, th2, max_peels,
+                     capacity, st, amps, th_amps, info, base + m.peel_off,
+                     m.bytes - m.peel_off, s, wait_limit_ns());
+}
+
+int ks_features(const float* Xres, const int64_t* st, const float* amps,
+                const float* W, const int64_t* iCC, const int64_t* iU,
+                const float* Ucc, int64_t C, int64_t L, int64_t K, int64_t P,
+                int64_t nt, int64_t nC, int64_t n_spikes, float* tF, void* stream) {
+  return launch_features(Xres, st, amps, W, iCC, iU, Ucc, C, L, K, P, nt, nC, n_spikes,
+                         tF, static_cast<cudaStream_t>(stream));
+}
+
+int ks_template_channels(const float* U, const int64_t* iCC, int64_t K, int64_t P,
+                         int64_t C, int64_t nC, int64_t* iU, float* Ucc,
+                         void* stream) {
+  return launch_template_channels(U, iCC, K, P, C, nC, iU, Ucc,
+                                  static_cast<cudaStream_t>(stream));
+}
+
+size_t ks_ctc_workspace_size(int64_t K, int64_t P, int64_t C, int64_t nt) {
+  return ctc_workspace_size(K, P, C, nt);
+}
+
+int ks_ctc(const float* U, const float* W, int64_t K, int64_t P, int64_t C,
+           int64_t nt, float* ctc, void* workspace, size_t workspace_bytes,
+           void* stream) {
+  return launch_ctc(U, W, K, P, C, nt, ctc, workspace, workspace_bytes,
+                    static_cast<cudaStream_t>(stream));
+}
+
+int ks_selftest_wait(int64_t timeout_ns, int* status, void* stream) {
+  if (!status || timeout_ns <= 0 || timeout_ns > 10000000000LL)
+    return fail(KS_ERR_ARG, "ks_selftest_wait: need 0 < timeout_ns <= 1e10 and a status pointer");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the flag lives in the status word's neighbour: status[1] is cleared and
+  // never set, so the wait can only end through its limit
+  KS_CUDA(cudaMemsetAsync(status, 0, 2 * sizeof(int), s));
+  ks_wait_never_kernel<<<1, 1, 0, s>>>((unsigned long long)timeout_ns, status, status + 1);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,103 @@
+// Shared helpers of the sm_100a kernels: error plumbing, device-wide barrier
+// with a bounded wait, timers and exact-rounding arithmetic.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/ks_b200.h"
+
+namespace ks {
+
+// Message of the last failure on the calling host thread.
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define KS_CUDA(call)                                        \
+  do {                                                       \
+    cudaError_t _e = (call);                                 \
+    if (_e != cudaSuccess) return ::ks::cuda_fail(_e, #call); \
+  } while (0)
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Per-device properties cached on first use.
+struct DeviceInfo {
+  int device = -1;
+  int sm_count = 0;
+  int cc_major = 0, cc_minor = 0;
+  size_t smem_optin = 0;
+};
+int device_info(DeviceInfo* out);
+
+// Simple bump allocator over a caller workspace.
+struct Carve {
+  char* base;
+  size_t used = 0;
+  explicit Carve(void* p) : base(static_cast<char*>(p)) {}
+  template <typename T>
+  T* take(size_t n) {
+    T* p = reinterpret_cast<T*>(base ? base + used : nullptr);
+    used = align256(used + n * sizeof(T));
+    return p;
+  }
+};
+
+// Default limit of every device-side wait (ns of %globaltimer).
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+
+}  // namespace ks
+
+// ---------------------------------------------------------------- device side
+
+__device__ __forceinline__ unsigned long long ks_globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned ks_ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ int ks_ld_volatile(const int* p) {
+  return *reinterpret_cast<const volatile int*>(p);
+}
+
+// Device-wide barrier for a cooperative (co-resident) grid.  bar[0] counts
+// arrivals, bar[1] is the generation.  A wait that exceeds limit_ns records
+// KS_ERR_TIMEOUT in *err and returns; every caller then sees the error flag
+// and leaves its loop, so no block waits without bound.
+// Returns true when no error is recorded.
+__device__ __forceinline__ bool ks_grid_sync(unsigned* bar, unsigned nblocks,
+                                             int* err,
+                                             unsigned long long limit_ns) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned gen = ks_ld_acquire(&bar[1]);
+    __threadfence();
+    unsigned arrived = atomicAdd(&bar[0], 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(&bar[0], 0u);
+      __threadfence();
+      atomicAdd(&bar[1], 1u);
+    } else {
+      unsigned long long t0 = ks_globaltimer();
+      while (ks_ld_acquire(&bar[1]) == gen) {
+        __nanosleep(64);
+        if (ks_globaltimer() - t0 > limit_ns) {
+          atomicCAS(err, 0, KS_ERR_TIMEOUT);
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ks_ld_volatile(err) == 0;
+}

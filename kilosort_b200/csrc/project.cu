@@ -1,0 +1,358 @@
+// Score projection B[k, tau] = sum_{p,c} U[k,p,c] * Y[c,p,tau],
+// Y[c,p,tau] = sum_t W[p,t] X[c, tau - nt/2 + t] (zero padding),
+// i.e. kilosort/template_matching.py:180-181 (conv1d then einsum).
+//
+// Layout in HBM (per call, carved from the caller's workspace)
+//   Yt  [Lpad, Q] temporal projection, q = c*P + p contiguous ("K-major" for
+//       the contraction), Lpad = roundup(L, 128), Q = roundup(roundup(C,16)*P, 64)
+//       float32 (FP32 form) or two bf16 planes hi/lo (split form)
+//   Uq  [Kpad, Q] templates in the same q order, zero padded; float32 or bf16 hi/lo
+//   B   [K, ldb] float32 output
+//
+// Kernels
+//   ks_prep_templates  nm[k] and Uq (both precisions)
+//   ks_temporal        X -> Yt: each thread owns 8 consecutive samples of one
+//                      channel and all P components (8*P FMA per tap, one
+//                      shared-memory load of X per tap); output staged in
+//                      shared memory and written as contiguous rows
+//   ks_sgemm_tn        FP32 SIMT contraction, 128x128x16 tiles, 8x8 per thread,
+//                      register double buffering; tile order puts the template
+//                      tiles of one time tile next to each other so each Yt tile
+//                      is read from HBM once
+#include "ks_common.cuh"
+#include "project.cuh"
+
+#include <cuda_bf16.h>
+
+namespace ks {
+
+// ------------------------------------------------------------------ prep
+__global__ void ks_template_energy_kernel(const float* __restrict__ U, int K,
+                                          int P, int C, float* __restrict__ nm) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= K) return;
+  const float* u = U + (long long)warp * P * C;
+  float tot = 0.f;
+  for (int p = 0; p < P; ++p) {
+    float s = 0.f;
+    for (int c = lane; c < C; c += 32) s = __fadd_rn(s, __fmul_rn(u[p * C + c], u[p * C + c]));
+    for (int o = 16; o; o >>= 1) s = __fadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+    tot = __fadd_rn(tot, s);
+  }
+  if (lane == 0) nm[warp] = tot;
+}
+
+__global__ void ks_reorder_templates_kernel(const float* __restrict__ U, int K,
+                                            int P, int C, int Kpad, int Q,
+                                            float* __restrict__ Uf,
+                                            __nv_bfloat16* __restrict__ Uhi,
+                                            __nv_bfloat16* __restrict__ Ulo) {
+  const long long n = (long long)Kpad * Q;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(e / Q);
+    const int q = (int)(e - (long long)k * Q);
+    const int c = q / P, p = q - (q / P) * P;
+    float v = 0.f;
+    if (k < K && c < C) v = U[((long long)k * P + p) * C + c];
+    if (Uf) Uf[e] = v;
+    if (Uhi) {
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      Uhi[e] = h;
+      Ulo[e] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+  }
+}
+
+// ------------------------------------------------------------------ temporal
+constexpr int kTT = 128;   // samples per tile
+constexpr int kCG = 16;    // channels per tile
+constexpr int kPMax = 8;
+
+template <int PP>
+__global__ void __launch_bounds__(256)
+ks_temporal_kernel(const float* __restrict__ X, const float* __restrict__ W,
+                   int C, int L, int nt, int Q, float* __restrict__ Yf,
+                   __nv_bfloat16* __restrict__ Yhi, __nv_bfloat16* __restrict__ Ylo) {
+  extern __shared__ __align__(16) float sm[];
+  const int xw = kTT + nt + 7;              // X window per channel (+ slack)
+  float* sX = sm;                           // [kCG][xw]
+  float* sW = sX + kCG * xw;                // [nt][PP]  (tap-major)
+  float* sY = sW + ((nt * PP + 3) & ~3);    // [kTT][kCG*PP]
+  const int tau0 = blockIdx.x * kTT;
+  const int cg0 = blockIdx.y * kCG;
+  const int half = nt / 2;
+  for (int i = threadIdx.x; i < kCG * xw; i += 256) {
+    const int cl = i / xw, u = i - cl * xw;
+    const int c = cg0 + cl, t = tau0 - half + u;
+    sX[i] = (c < C && t >= 0 && t < L) ? X[(long long)c * L + t] : 0.f;
+  }
+  for (int i = threadIdx.x; i < nt * PP; i += 256) {
+    const int t = i / PP, p = i - t * PP;
+    sW[i] = W[p * nt + t];
+  }
+  __syncthreads();
+  const int cl = threadIdx.x & (kCG - 1);
+  const int g = threadIdx.x / kCG;          // 16 groups of 8 samples
+  const float* xs = sX + cl * xw + g * 8;
+  float acc[8][PP];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int p = 0; p < PP; ++p) acc[i][p] = 0.f;
+  float win[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) win[i] = xs[i];
+  for (int t = 0; t < nt; ++t) {
+    float w[PP];
+#pragma unroll
+    for (int p = 0; p < PP; ++p) w[p] = sW[t * PP + p];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int p = 0; p < PP; ++p) acc[i][p] = fmaf(w[p], win[i], acc[i][p]);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) win[i] = win[i + 1];
+    win[7] = xs[t + 8];
+  }
+  const int row = kCG * PP;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int p = 0; p < PP; ++p) sY[(g * 8 + i) * row + cl * PP + p] = acc[i][p];
+  __syncthreads();
+  const long long q0 = (long long)cg0 * PP;
+  for (int e = threadIdx.x; e < kTT * row; e += 256) {
+    const int r = e / row, q = e - r * row;
+    const long long o = (long long)(tau0 + r) * Q + q0 + q;
+    const float v = sY[e];
+    if (Yf) Yf[o] = v;
+    if (Yhi) {
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      Yhi[o] = h;
+      Ylo[o] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+  }
+}
+
+size_t temporal_smem(int nt, int P) {
+  const int xw = kTT + nt + 7;
+  return sizeof(float) * ((size_t)kCG * xw + ((nt * P + 3) & ~3) + (size_t)kTT * kCG * P);
+}
+
+// ------------------------------------------------------------------ FP32 GEMM
+constexpr int kBM = 128, kBN = 128, kBK = 16;
+
+// C[m, n] = sum_q A[m, q] * Bt[n, q]; A is [>= tiles_m*128, Kd], Bt is
+// [>= tiles_n*128, Kd] (both zero padded), Kd % 16 == 0.  Stores m < M, n < N.
+__global__ void __launch_bounds__(256, 2)
+ks_sgemm_tn_kernel(const float* __restrict__ A, const float* __restrict__ Bt,
+                   float* __restrict__ Cm, int M, int N, int Kd, long long ldc,
+                   int tiles_m) {
+  __shared__ __align__(16) float As[2][kBK][kBM + 4];
+  __shared__ __align__(16) float Bs[2][kBK][kBN + 4];
+  const int tid = threadIdx.x;
+  const int tm = blockIdx.x % tiles_m;
+  const int tn = blockIdx.x / tiles_m;
+  const long long m0 = (long long)tm * kBM, n0 = (long long)tn * kBN;
+  const int tx = tid & 15, ty = tid >> 4;
+  // loader mapping: two float4 per operand per thread
+  int lrow[2], lc4[2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int idx = tid + i * 256;
+    lrow[i] = idx >> 2;
+    lc4[i] = idx & 3;
+  }
+  float4 ra[2], rb[2];
+  auto gload = [&](int k0) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      ra[i] = *reinterpret_cast<const float4*>(A + (m0 + lrow[i]) * Kd + k0 + lc4[i] * 4);
+      rb[i] = *reinterpret_cast<const float4*>(Bt + (n0 + lrow[i]) * Kd + k0 + lc4[i] * 4);
+    }
+  };
+  auto sstore = [&](int buf) {
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int kk = lc4[i] * 4;
+      As[buf][kk + 0][lrow[i]] = ra[i].x;
+      As[buf][kk + 1][lrow[i]] = ra[i].y;
+      As[buf][kk + 2][lrow[i]] = ra[i].z;
+      As[buf][kk + 3][lrow[i]] = ra[i].w;
+      Bs[buf][kk + 0][lrow[i]] = rb[i].x;
+      Bs[buf][kk + 1][lrow[i]] = rb[i].y;
+      Bs[buf][kk + 2][lrow[i]] = rb[i].z;
+      Bs[buf][kk + 3][lrow[i]] = rb[i].w;
+    }
+  };
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+
+  gload(0);
+  sstore(0);
+  __syncthreads();
+  const int nk = Kd / kBK;
+  for (int kt = 0; kt < nk; ++kt) {
+    const int buf = kt & 1;
+    if (kt + 1 < nk) gload((kt + 1) * kBK);
+#pragma unroll
+    for (int kk = 0; kk < kBK; ++kk) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][kk][64 + ty * 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][kk][tx * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][kk][64 + tx * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+    if (kt + 1 < nk) sstore(buf ^ 1);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const long long m = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+    if (m >= M) continue;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const long long n = n0 + h * 64 + tx * 4;
+      float* dst = Cm + m * ldc + n;
+      const float* v = &acc[i][h * 4];
+      if (n + 3 < N && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0)) {
+        *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+      } else {
+        for (int e = 0; e < 4; ++e)
+          if (n + e < N) dst[e] = v[e];
+      }
+    }
+  }
+}
+
+int sgemm_tn(const float* A, const float* Bt, float* Cm, int64_t M, int64_t N,
+             int64_t Kd, int64_t ldc, cudaStream_t stream) {
+  if (Kd % kBK) return fail(KS_ERR_ARG, "sgemm_tn: Kd must be a multiple of 16");
+  const int tiles_m = (int)((M + kBM - 1) / kBM);
+  const int tiles_n = (int)((N + kBN - 1) / kBN);
+  const long long nblocks = (long long)tiles_m * tiles_n;
+  if (nblocks > 0x7fffffffLL) return fail(KS_ERR_UNSUPPORTED, "sgemm_tn: too many tiles");
+  ks_sgemm_tn_kernel<<<(unsigned)nblocks, 256, 0, stream>>>(A, Bt, Cm, (int)M, (int)N,
+                                                            (int)Kd, ldc, tiles_m);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
+// ------------------------------------------------------------------ driver
+ProjLayout proj_layout(int64_t C, int64_t L, int64_t K, int64_t P, int precision) {
+  ProjLayout l;
+  l.Q = round_up(round_up(C, kCG) * P, 64);
+  l.Lpad = round_up(L, 128);
+  l.Kpad = round_up(K, 128);
+  Carve cv(nullptr);
+  if (precision == KS_PROJ_FP32) {
+    cv.take<float>((size_t)l.Kpad * l.Q);
+    cv.take<float>((size_t)l.Lpad * l.Q);
+  } else {
+    cv.take<__nv_bfloat16>((size_t)l.Kpad * l.Q * 2);
+    cv.take<__nv_bfloat16>((size_t)l.Lpad * l.Q * 2);
+  }
+  l.bytes = cv.used;
+  return l;
+}
+
+int launch_template_energy(const float* U, int64_t K, int64_t P, int64_t C,
+                           float* nm, cudaStream_t stream) {
+  if (!U || !nm || K < 1 || P < 1 || C < 1) return fail(KS_ERR_ARG, "template_energy: bad args");
+  const int threads = 256;
+  const long long blocks = (K * 32 + threads - 1) / threads;
+  ks_template_energy_kernel<<<(unsigned)blocks, threads, 0, stream>>>(U, (int)K, (int)P, (int)C, nm);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
+int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
+                    int64_t P, int64_t nt, int64_t Q, int64_t Lpad, float* Yf,
+                    __nv_bfloat16* Yhi, __nv_bfloat16* Ylo, cudaStream_t stream) {
+  const size_t smem = temporal_smem((int)nt, (int)P);
+  dim3 grid((unsigned)(Lpad / kTT), (unsigned)((C + kCG - 1) / kCG));
+#define KS_TEMPORAL_CASE(PPV)                                                              \
+  case PPV: {                                                                              \
+    KS_CUDA(cudaFuncSetAttribute(ks_temporal_kernel<PPV>,                                  \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    ks_temporal_kernel<PPV><<<grid, 256, smem, stream>>>(X, W, (int)C, (int)L, (int)nt,    \
+                                                         (int)Q, Yf, Yhi, Ylo);            \
+    break;                                                                                 \
+  }
+  switch (P) {
+    KS_TEMPORAL_CASE(1)
+    KS_TEMPORAL_CASE(2)
+    KS_TEMPORAL_CASE(3)
+    KS_TEMPORAL_CASE(4)
+    KS_TEMPORAL_CASE(5)
+    KS_TEMPORAL_CASE(6)
+    KS_TEMPORAL_CASE(7)
+    KS_TEMPORAL_CASE(8)
+    default:
+      return fail(KS_ERR_UNSUPPORTED, "project: n_pcs must be 1..8");
+  }
+#undef KS_TEMPORAL_CASE
+  KS_CUDA(cudaGetLastError());
+  // q columns past the last channel group are padding: zero them
+  const int64_t qused = round_up(C, kCG) * P;
+  if (qused < Q) {
+    if (Yf) KS_CUDA(cudaMemset2DAsync(Yf + qused, Q * sizeof(float), 0, (Q - qused) * sizeof(float), Lpad, stream));
+    if (Yhi) {
+      KS_CUDA(cudaMemset2DAsync(Yhi + qused, Q * 2, 0, (Q - qused) * 2, Lpad, stream));
+      KS_CUDA(cudaMemset2DAsync(Ylo + qused, Q * 2, 0, (Q - qused) * 2, Lpad, stream));
+    }
+  }
+  return KS_OK;
+}
+
+int launch_project(const float* X, const float* U, const float* W, int64_t C,
+                   int64_t L, int64_t K, int64_t P, int64_t nt, int precision,
+                   float* B, int64_t ldb, void* ws, size_t ws_bytes,
+                   cudaStream_t stream) {
+  if (!X || !U || !W || !B) return fail(KS_ERR_ARG, "ks_project: null pointer");
+  if (C < 1 || L < 1 || K < 1 || P < 1 || nt < 1 || (nt % 2) == 0)
+    return fail(KS_ERR_ARG, "ks_project: need C,L,K,P >= 1 and odd nt");
+  if (P > kPMax) return fail(KS_ERR_UNSUPPORTED, "ks_project: n_pcs must be <= 8");
+  if (nt > 1023) return fail(KS_ERR_UNSUPPORTED, "ks_project: nt must be <= 1023");
+  if (ldb < L) return fail(KS_ERR_ARG, "ks_project: ldb < L");
+  if (precision != KS_PROJ_FP32 && precision != KS_PROJ_BF16X3)
+    return fail(KS_ERR_ARG, "ks_project: unknown precision");
+  const ProjLayout lay = proj_layout(C, L, K, P, precision);
+  if (!ws || ws_bytes < lay.bytes) return fail(KS_ERR_WORKSPACE, "ks_project: workspace too small");
+  Carve cv(ws);
+  const int reorder_blocks = (int)std::min<int64_t>(4096, (lay.Kpad * lay.Q + 255) / 256);
+  if (precision == KS_PROJ_FP32) {
+    float* Uq = cv.take<float>((size_t)lay.Kpad * lay.Q);
+    float* Yt = cv.take<float>((size_t)lay.Lpad * lay.Q);
+    ks_reorder_templates_kernel<<<reorder_blocks, 256, 0, stream>>>(
+        U, (int)K, (int)P, (int)C, (int)lay.Kpad, (int)lay.Q, Uq, nullptr, nullptr);
+    KS_CUDA(cudaGetLastError());
+    int rc = launch_temporal(X, W, C, L, P, nt, lay.Q, lay.Lpad, Yt, nullptr, nullptr, stream);
+    if (rc) return rc;
+    return sgemm_tn(Uq, Yt, B, K, L, lay.Q, ldb, stream);
+  }
+  __nv_bfloat16* Uhl = cv.take<__nv_bfloat16>((size_t)lay.Kpad * lay.Q * 2);
+  __nv_bfloat16* Yhl = cv.take<__nv_bfloat16>((size_t)lay.Lpad * lay.Q * 2);
+  __nv_bfloat16* Uhi = Uhl;
+  __nv_bfloat16* Ulo = Uhl + (size_t)lay.Kpad * lay.Q;
+  __nv_bfloat16* Yhi = Yhl;
+  __nv_bfloat16* Ylo = Yhl + (size_t)lay.Lpad * lay.Q;
+  ks_reorder_templates_kernel<<<reorder_blocks, 256, 0, stream>>>(
+      U, (int)K, (int)P, (int)C, (int)lay.Kpad, (int)lay.Q, nullptr, Uhi, Ulo);
+  KS_CUDA(cudaGetLastError());
+  int rc = launch_temporal(X, W, C, L, P, nt, lay.Q, lay.Lpad, nullptr, Yhi, Ylo, stream);
+  if (rc) return rc;
+  return gemm_bf16x3(Uhi, Ulo, Yhi, Ylo, B, K, L, lay.Q, lay.Kpad, lay.Lpad, ldb, stream);
+}
+
+}  // namespace ks

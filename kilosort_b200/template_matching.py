@@ -1,0 +1,356 @@
+"""Drop-in replacements for ``kilosort.template_matching`` on a B200.
+
+Same signatures, argument meanings, outputs and error behaviour as the
+reference functions (kilosort/template_matching.py):
+
+* ``prepare_extract(xc, yc, U, nC, position_limit, device)``   (:14-53)
+* ``extract(ops, bfile, U, device, progress_bar)``              (:56-126)
+* ``prepare_matching(ops, U)``                                  (:155-167)
+* ``run_matching(ops, X, U, ctc, device)``                      (:170-244)
+
+PyTorch only holds device memory and supplies the current CUDA stream; every
+computation runs in the sm_100a kernels of ``libks_b200.so``.  There is no CPU
+path: inputs must be float32 CUDA tensors on a B200.
+
+Extra ``ops`` keys understood here (the reference ignores them):
+``projection`` -- ``"fp32"`` (plain FP32 contraction, the default) or
+``"bf16x3"`` (split-BF16 on tensor cores); ``spike_capacity`` -- spike rows
+per batch (default 100000, the reference's fixed buffer size).
+"""
+from __future__ import annotations
+
+import logging
+
+import numpy as np
+import torch
+
+from . import _lib
+
+logger = logging.getLogger(__name__)
+
+DEFAULT_CAPACITY = 100000
+_PROJECTIONS = {"fp32": _lib.KS_PROJ_FP32, "bf16x3": _lib.KS_PROJ_BF16X3}
+_default_projection = "fp32"
+
+
+def set_default_projection(name: str) -> None:
+    """Select the projection used when ``ops`` has no ``projection`` key."""
+    global _default_projection
+    if name not in _PROJECTIONS:
+        raise ValueError(f"projection must be one of {sorted(_PROJECTIONS)}")
+    _default_projection = name
+
+
+def _projection(ops) -> int:
+    name = ops.get("projection", _default_projection) if hasattr(ops, "get") else _default_projection
+    if name not in _PROJECTIONS:
+        raise ValueError(f"ops['projection'] must be one of {sorted(_PROJECTIONS)}")
+    return _PROJECTIONS[name]
+
+
+def _ptr(t: torch.Tensor) -> int:
+    return t.data_ptr()
+
+
+def _stream(device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _need(t, name, dtype=torch.float32, ndim=None):
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a torch.Tensor")
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor (this path has no CPU fallback)")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if ndim is not None and t.dim() != ndim:
+        raise ValueError(f"{name} must have {ndim} dims, got shape {tuple(t.shape)}")
+    return t.contiguous()
+
+
+class _Workspace:
+    """One growable device scratch buffer per device, reused across calls."""
+
+    def __init__(self):
+        self._bufs = {}
+
+    def get(self, device, nbytes: int) -> torch.Tensor:
+        key = (device.type, device.index)
+        buf = self._bufs.get(key)
+        if buf is None or buf.numel() < nbytes:
+            self._bufs.pop(key, None)
+            buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+            self._bufs[key] = buf
+        return buf
+
+
+_ws = _Workspace()
+
+
+def th2_of(Th) -> float:
+    """Th_learned**2 as the reference's float32 comparison sees it."""
+    return float(np.float32(float(Th) ** 2))
+
+
+# ------------------------------------------------------------------ building blocks
+def template_energy(U: torch.Tensor) -> torch.Tensor:
+    """nm[k] = sum_{p,c} U[k,p,c]^2 (kilosort/template_matching.py:176)."""
+    U = _need(U, "U", ndim=3)
+    K, P, Cn = U.shape
+    nm = torch.empty(K, dtype=torch.float32, device=U.device)
+    lib = _lib.load()
+    _lib.check(lib.ks_template_energy(_ptr(U), K, P, Cn, _ptr(nm), _stream(U.device)),
+               "ks_template_energy")
+    return nm
+
+
+def project_scores(X, U, W, nt, projection="fp32"):
+    """Score matrix B [K, L] (kilosort/template_matching.py:180-181)."""
+    X = _need(X, "X", ndim=2)
+    U = _need(U, "U", ndim=3)
+    W = _need(W, "wPCA", ndim=2)
+    Cn, L = X.shape
+    K, P, Cu = U.shape
+    if Cu != Cn or W.shape != (P, nt):
+        raise ValueError("shape mismatch between X, U and wPCA")
+    prec = _PROJECTIONS[projection]
+    lib = _lib.load()
+    ldb = ((L + 63) // 64) * 64
+    B = torch.empty((K, ldb), dtype=torch.float32, device=X.device)
+    nbytes = lib.ks_project_workspace_size(Cn, L, K, P, prec)
+    ws = _ws.get(X.device, nbytes)
+    _lib.check(lib.ks_project(_ptr(X), _ptr(U), _ptr(W), Cn, L, K, P, nt, prec,
+                              _ptr(B), ldb, _ptr(ws), ws.numel(), _stream(X.device)),
+               "ks_project")
+    return B[:, :L]
+
+
+def _info_status(info, what):
+    n, status, iters, need = (int(v) for v in info.tolist())
+    if status == _lib.KS_ERR_OVERFLOW:
+        raise RuntimeError(
+            f"{what}: {need} spikes in one batch exceed the spike buffer "
+            f"(capacity {n} written so far); raise ops['spike_capacity']")
+    if status != _lib.KS_OK:
+        raise _lib.KilosortB200Error(status, f"{what}: device status {status} "
+                                     f"({_lib.status_message(status)})")
+    return n, iters
+
+
+def peel(B, Xres, U, W, ctc, nm, Th, nt, max_peels, capacity=DEFAULT_CAPACITY):
+    """Greedy peel on a given score matrix, in place on B and Xres.
+
+    Returns (st [N,2] int64, amps [N,1], th_amps [N,1], iterations), in the
+    order of kilosort/template_matching.py:183-244.
+    """
+    if not (isinstance(B, torch.Tensor) and B.is_cuda and B.dtype == torch.float32
+            and B.dim() == 2 and B.stride(1) == 1 and B.stride(0) >= B.shape[1]):
+        raise ValueError("B must be a float32 CUDA matrix with contiguous rows")
+    ldb = B.stride(0)
+    Xres = _need(Xres, "Xres", ndim=2)
+    U = _need(U, "U", ndim=3)
+    W = _need(W, "wPCA", ndim=2)
+    ctc = _need(ctc, "ctc", ndim=3)
+    nm = _need(nm, "nm", ndim=1)
+    K, P, Cn = U.shape
+    L = Xres.shape[1]
+    if B.shape != (K, L) or ctc.shape != (K, K, 2 * nt + 1):
+        raise ValueError("shape mismatch between B, U, ctc and Xres")
+    dev = Xres.device
+    st = torch.zeros((capacity, 2), dtype=torch.int64, device=dev)
+    amps = torch.zeros((capacity, 1), dtype=torch.float32, device=dev)
+    th_amps = torch.zeros((capacity, 1), dtype=torch.float32, device=dev)
+    info = torch.zeros(4, dtype=torch.int64, device=dev)
+    lib = _lib.load()
+    ws = _ws.get(dev, lib.ks_peel_workspace_size(L, K))
+    _lib.check(lib.ks_peel(_ptr(B), ldb, _ptr(Xres), _ptr(U), _ptr(W), _ptr(ctc), _ptr(nm),
+                           Cn, L, K, P, nt, th2_of(Th), int(max_peels), int(capacity),
+                           _ptr(st), _ptr(amps), _ptr(th_amps), _ptr(info),
+                           _ptr(ws), ws.numel(), _stream(dev)), "ks_peel")
+    n, iters = _info_status(info, "ks_peel")
+    return st[:n], amps[:n], th_amps[:n], iters
+
+
+# ------------------------------------------------------------------ drop-in API
+def run_matching(ops, X, U, ctc, device=torch.device("cuda")):
+    """Greedy template matching of one padded batch.
+
+    Same contract as kilosort/template_matching.py:170-244: returns
+    ``(st [N,2] int64, amps [N,1] float32, th_amps [N,1] float32, Xres [C,L])``
+    with spikes in (iteration, time) order; ``X`` is not modified.
+    """
+    Th = ops["Th_learned"]
+    nt = int(ops["nt"])
+    max_peels = int(ops["max_peels"])
+    W = _need(ops["wPCA"], "ops['wPCA']", ndim=2)
+    X = _need(X, "X", ndim=2)
+    U = _need(U, "U", ndim=3)
+    ctc = _need(ctc, "ctc", ndim=3)
+    Cn, L = X.shape
+    K, P, Cu = U.shape
+    if Cu != Cn:
+        raise ValueError(f"U has {Cu} channels but X has {Cn}")
+    if W.shape != (P, nt):
+        raise ValueError(f"wPCA must be [{P}, {nt}], got {tuple(W.shape)}")
+    if ctc.shape != (K, K, 2 * nt + 1):
+        raise ValueError(f"ctc must be [{K}, {K}, {2 * nt + 1}], got {tuple(ctc.shape)}")
+    capacity = int(ops.get("spike_capacity", DEFAULT_CAPACITY)) if hasattr(ops, "get") \
+        else DEFAULT_CAPACITY
+    prec = _projection(ops)
+    dev = X.device
+    st = torch.zeros((capacity, 2), dtype=torch.int64, device=dev)
+    amps = torch.zeros((capacity, 1), dtype=torch.float32, device=dev)
+    th_amps = torch.zeros((capacity, 1), dtype=torch.float32, device=dev)
+    Xres = torch.empty_like(X)
+    info = torch.zeros(4, dtype=torch.int64, device=dev)
+    lib = _lib.load()
+    ws = _ws.get(dev, lib.ks_run_matching_workspace_size(Cn, L, K, P, prec))
+    _lib.check(lib.ks_run_matching(_ptr(X), _ptr(U), _ptr(W), _ptr(ctc), Cn, L, K, P, nt,
+                                   th2_of(Th), max_peels, prec, capacity, _ptr(st),
+                                   _ptr(amps), _ptr(th_amps), _ptr(Xres), _ptr(info),
+                                   _ptr(ws), ws.numel(), _stream(dev)), "ks_run_matching")
+    n, _ = _info_status(info, "run_matching")
+    return st[:n], amps[:n], th_amps[:n], Xres
+
+
+def prepare_matching(ops, U):
+    """Template cross-correlations ctc [K, K, 2nt+1] (template_matching.py:155-167)."""
+    nt = int(ops["nt"])
+    W = _need(ops["wPCA"], "ops['wPCA']", ndim=2)
+    U = _need(U, "U", ndim=3)
+    K, P, Cn = U.shape
+    ctc = torch.empty((K, K, 2 * nt + 1), dtype=torch.float32, device=U.device)
+    lib = _lib.load()
+    ws = _ws.get(U.device, lib.ks_ctc_workspace_size(K, P, Cn, nt))
+    _lib.check(lib.ks_ctc(_ptr(U), _ptr(W), K, P, Cn, nt, _ptr(ctc), _ptr(ws), ws.numel(),
+                          _stream(U.device)), "ks_ctc")
+    return ctc
+
+
+def prepare_extract(xc, yc, U, nC, position_limit, device=torch.device("cuda")):
+    """Nearest channels, masks, peak channels and loadings (template_matching.py:14-53).
+
+    The channel neighbourhoods are host-side numpy, as in the reference; the
+    per-template peak channel ``iU`` and loadings ``Ucc`` come from the GPU.
+    """
+    ds = (xc - xc[:, np.newaxis]) ** 2 + (yc - yc[:, np.newaxis]) ** 2
+    iCC = np.argsort(ds, 0)[:nC]
+    iCC = torch.from_numpy(iCC).to(device)
+    iCC_mask = np.sort(ds, 0)[:nC] < position_limit ** 2
+    iCC_mask = torch.from_numpy(iCC_mask).to(device)
+    U = _need(U, "U", ndim=3)
+    K, P, Cn = U.shape
+    iCCd = iCC.to(U.device).contiguous()
+    iU = torch.empty(K, dtype=torch.int64, device=U.device)
+    Ucc = torch.empty((nC, K, P), dtype=torch.float32, device=U.device)
+    lib = _lib.load()
+    _lib.check(lib.ks_template_channels(_ptr(U), _ptr(iCCd), K, P, Cn, nC, _ptr(iU),
+                                        _ptr(Ucc), _stream(U.device)),
+               "ks_template_channels")
+    return iCC, iCC_mask, iU, Ucc
+
+
+def spike_features(Xres, st, amps, W, iCC, iU, Ucc):
+    """Per-spike PC features [N, nC, P] (template_matching.py:85-86, 108)."""
+    Xres = _need(Xres, "Xres", ndim=2)
+    W = _need(W, "wPCA", ndim=2)
+    st = _need(st, "st", dtype=torch.int64, ndim=2)
+    amps = _need(amps, "amps").reshape(-1)
+    iCC = _need(iCC, "iCC", dtype=torch.int64, ndim=2)
+    iU = _need(iU, "iU", dtype=torch.int64, ndim=1)
+    Ucc = _need(Ucc, "Ucc", ndim=3)
+    nC, K, P = Ucc.shape
+    Cn, L = Xres.shape
+    nt = W.shape[1]
+    N = st.shape[0]
+    tF = torch.empty((N, nC, P), dtype=torch.float32, device=Xres.device)
+    if N == 0:
+        return tF
+    lib = _lib.load()
+    _lib.check(lib.ks_features(_ptr(Xres), _ptr(st), _ptr(amps), _ptr(W), _ptr(iCC),
+                               _ptr(iU), _ptr(Ucc), Cn, L, K, P, nt, nC, N, _ptr(tF),
+                               _stream(Xres.device)), "ks_features")
+    return tF
+
+
+def extract(ops, bfile, U, device=torch.device("cuda"), progress_bar=None):
+    """Match every batch of ``bfile`` and collect spikes and PC features.
+
+    Same contract as kilosort/template_matching.py:56-126: returns
+    ``(st [N,3] float64 numpy (time, template, th_amp), tF [N,nC,P] CPU
+    tensor, ops)`` sorted by time, and stores ``iCC``, ``iCC_mask``, ``iU``
+    in ``ops``.
+    """
+    try:
+        from tqdm import tqdm
+    except ImportError:  # pragma: no cover
+        tqdm = None
+    nC = ops["settings"]["nearest_chans"]
+    position_limit = ops["settings"]["position_limit"]
+    iCC, iCC_mask, iU, Ucc = prepare_extract(ops["xc"], ops["yc"], U, nC,
+                                             position_limit, device=device)
+    ops["iCC"] = iCC
+    ops["iCC_mask"] = iCC_mask
+    ops["iU"] = iU
+    nt = ops["nt"]
+    ctc = prepare_matching(ops, U)
+    st = np.zeros((10 ** 6, 3), "float64")
+    tF = torch.zeros((10 ** 6, nC, ops["settings"]["n_pcs"]))
+    k = 0
+    batches = np.arange(bfile.n_batches, dtype=np.int64)
+    prog = tqdm(batches, miniters=200 if progress_bar else None,
+                mininterval=60 if progress_bar else None) if tqdm else batches
+    W = ops["wPCA"].contiguous()
+    iCCd = iCC.to(U.device).contiguous()
+    ibatch = -1
+    try:
+        for ibatch in prog:
+            if ibatch % 100 == 0 and torch.cuda.is_available():
+                logger.debug(f"Batch {ibatch}: {torch.cuda.memory_allocated() / 2**30:.2f} GiB allocated")
+            X = bfile.padded_batch_to_torch(ibatch, ops)
+            stt, amps, th_amps, Xres = run_matching(ops, X, U, ctc, device=device)
+            xfeat = spike_features(Xres, stt, amps, W, iCCd, iU, Ucc)   # [N, nC, P]
+            if ibatch == 0:
+                neg = (stt[:, 0] - nt - nt // 2 + ops["nt0min"]) < 0
+                stt = stt[~neg, :]
+                xfeat = xfeat[~neg]
+                amps = amps[~neg, :]
+                th_amps = th_amps[~neg, :]
+            nsp = len(stt)
+            if k + nsp > st.shape[0]:
+                st = np.concatenate((st, np.zeros_like(st)), 0)
+                tF = torch.cat((tF, torch.zeros_like(tF)), 0)
+            t_shift = ibatch * bfile.batch_downsampling * (ops["batch_size"])
+            stt = stt.double()
+            st[k:k + nsp, 0] = ((stt[:, 0] - nt) + t_shift).cpu().numpy() - nt // 2 + ops["nt0min"]
+            st[k:k + nsp, 1] = stt[:, 1].cpu().numpy()
+            st[k:k + nsp, 2] = th_amps.cpu().numpy().squeeze()
+            tF[k:k + nsp] = xfeat.cpu()
+            k += nsp
+            if progress_bar is not None:
+                progress_bar.emit(int((ibatch + 1) / bfile.n_batches * 100))
+    except Exception:
+        logger.exception(f"Error in kilosort_b200.extract on batch {ibatch}")
+        raise
+    isort = np.argsort(st[:k, 0])
+    st = st[isort]
+    tF = tF[isort]
+    return st, tF, ops
+
+
+def install(module=None):
+    """Route the reference's template matching through this implementation.
+
+    Replaces ``run_matching``, ``prepare_matching``, ``prepare_extract`` and
+    ``extract`` on ``kilosort.template_matching`` (or on ``module``).  The
+    reference's ``extract`` resolves ``run_matching`` as a module global, so
+    patching the attribute reroutes it as well.  Returns the patched module.
+    """
+    if module is None:
+        import importlib
+        module = importlib.import_module("kilosort.template_matching")
+    module.run_matching = run_matching
+    module.prepare_matching = prepare_matching
+    module.prepare_extract = prepare_extract
+    module.extract = extract
+    return module

@@ -1,0 +1,57 @@
+"""C-ABI library checks that need no GPU: it loads, exports every declared
+symbol, and its host-side queries answer."""
+import ctypes
+
+import pytest
+
+from kilosort_b200 import _lib
+
+
+def test_library_loads_and_exports_header_symbols():
+    lib = _lib.load()
+    declared = _lib.header_symbols()
+    assert len(declared) >= 15
+    for name in declared:
+        assert hasattr(lib, name), f"{name} declared in include/ks_b200.h but not exported"
+    # every binding we set up corresponds to a declared function
+    assert set(_lib.SIGNATURES) == set(declared)
+
+
+def test_status_strings_and_version():
+    lib = _lib.load()
+    assert lib.ks_version() >= 1
+    assert lib.ks_status_string(0) == b"ok"
+    assert b"overflow" in lib.ks_status_string(_lib.KS_ERR_OVERFLOW)
+    assert b"timed out" in lib.ks_status_string(_lib.KS_ERR_TIMEOUT)
+
+
+def test_workspace_queries():
+    lib = _lib.load()
+    C, L, K, P = 384, 60122, 600, 6
+    fp32 = lib.ks_project_workspace_size(C, L, K, P, _lib.KS_PROJ_FP32)
+    split = lib.ks_project_workspace_size(C, L, K, P, _lib.KS_PROJ_BF16X3)
+    # Yt: Lpad * Q floats (fp32) vs two bf16 planes -> same size; both > Y bytes
+    assert fp32 >= 60160 * 2304 * 4
+    assert split >= 60160 * 2304 * 4
+    assert lib.ks_peel_workspace_size(L, K) > 4 * L
+    total = lib.ks_run_matching_workspace_size(C, L, K, P, _lib.KS_PROJ_FP32)
+    assert total >= fp32 + K * L * 4
+    assert lib.ks_ctc_workspace_size(K, P, C, 61) >= (K * P) ** 2 * 4
+
+
+def test_peel_rejects_bad_arguments_before_touching_the_device():
+    lib = _lib.load()
+    # null pointers -> KS_ERR_ARG
+    rc = lib.ks_peel(None, 64, None, None, None, None, None, 4, 64, 2, 6, 61, 64.0,
+                     100, 10, None, None, None, None, None, 0, None)
+    assert rc == _lib.KS_ERR_ARG
+    assert b"null" in lib.ks_last_error()
+
+
+def test_python_layer_refuses_cpu_tensors():
+    import torch
+    import kilosort_b200 as kb
+    ops = dict(Th_learned=8.0, nt=61, max_peels=100, wPCA=torch.zeros(6, 61))
+    with pytest.raises(ValueError, match="CUDA"):
+        kb.run_matching(ops, torch.zeros(4, 200), torch.zeros(2, 6, 4),
+                        torch.zeros(2, 2, 123))
