@@ -2,8 +2,9 @@
 golden vectors made by the reference itself).
 
 Tolerances:
-* the peel given the reference's score matrix and energies is bit-exact in
-  st / amps / th_amps (integer and float outputs identical);
+* the peel given the same score matrix and energies as the oracle is
+  bit-exact in st, amps and the updated B; th_amps within 1 ulp (IEEE sqrt vs
+  the CPU build's vectorised sqrt);
 * full run_matching in FP32: (time, template) agreement >= 99.5 %, matched
   times exact, amplitude relative error <= 1e-4;
 * the residual Xres: |diff| <= 1e-5 * (1 + |x|);
@@ -59,7 +60,10 @@ def test_peel_bit_exact_given_same_scores(cuda_device, name):
                                   nm.to(DEV), ops["Th_learned"], nt, ops["max_peels"])
     np.testing.assert_array_equal(st.cpu().numpy(), st_o.numpy())
     np.testing.assert_array_equal(amps.cpu().numpy(), amps_o.numpy())
-    np.testing.assert_array_equal(th.cpu().numpy(), th_o.numpy())
+    # th_amps = sqrt(pooled): IEEE sqrt here (as the reference on CUDA); the
+    # reference's CPU build takes a vectorised sqrt that is 1 ulp off on ~0.7 %
+    # of inputs, so allow one ulp
+    np.testing.assert_array_max_ulp(th.cpu().numpy(), th_o.numpy(), maxulp=1)
     np.testing.assert_array_equal(Bd[:, :L].cpu().numpy(), Bo.numpy())
     np.testing.assert_allclose(Xres.cpu().numpy(), Xo.numpy(), rtol=0,
                                atol=1e-6 * (1 + np.abs(Xo.numpy()).max()))
