@@ -260,26 +260,24 @@ def main():
 
     e2e_ms, _ = timed(e2e_step, head)
 
-    # stage breakdown of one pass (projection vs peel) for the roofline
+    # stage breakdown of one pass with the kernels run_matching launches
+    # (projection into the tiled score layout, then the peel)
     stage = {"project": 0.0, "peel": 0.0}
     kused, nsp_total = 0, 0
-    ldb = ((L + 63) // 64) * 64
-    Bbuf = torch.empty((K, ldb), dtype=torch.float32, device=dev)
     nm = kb.template_energy(U)
+    ctcT = kb.transpose_ctc(ctc, NT)
     for X in Xs:
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        e[0].record()
-        B = kb.project_scores(X, U, W, NT, head)
-        e[1].record()
-        Bbuf[:, :L].copy_(B)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         Xres = X.clone()
-        e2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        e2[0].record()
-        st, amps, th, _ = kb.peel(Bbuf[:, :L], Xres, U, W, ctc, nm, TH, NT, 100)
-        e2[1].record()
+        e[0].record()
+        Bt = kb.project_scores(X, U, W, NT, head, tiled=True)
+        e[1].record()
+        e[2].record()
+        st, amps, th, _ = kb.peel(Bt, Xres, U, W, ctcT, nm, TH, NT, 100, ctc_transposed=True)
+        e[3].record()
         torch.cuda.synchronize()
         stage["project"] += e[0].elapsed_time(e[1])
-        stage["peel"] += e2[0].elapsed_time(e2[1])
+        stage["peel"] += e[2].elapsed_time(e[3])
         kused += len(torch.unique(st[:, 1]))
         nsp_total += len(st)
     nb = args.batches

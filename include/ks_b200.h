@@ -44,6 +44,14 @@ extern "C" {
 #define KS_ERR_UNSUPPORTED 6  /* device or shape not supported by this build */
 #define KS_ERR_DEGENERATE 7   /* exact score plateaus beyond the tie buffer */
 
+/* layout of the score matrix B */
+#define KS_B_ROWS 0           /* B[k][tau] row-major with leading dimension ldb */
+#define KS_B_TILED 1          /* Bt[tau/32][k][tau%32]: 32-column blocks, ceil(L/32)*K*32 floats */
+
+/* layout of the template cross-correlations */
+#define KS_CTC_JKL 0          /* ctc[j][k][lag], as prepare_matching returns it */
+#define KS_CTC_KJL 1          /* ctcT[k][j][lag] = ctc[j][k][lag] (ks_ctc_transpose) */
+
 /* projection precision */
 #define KS_PROJ_FP32 0        /* plain FP32 (SIMT) contraction */
 #define KS_PROJ_BF16X3 1      /* split-BF16 hi/lo, three tcgen05 MMAs, FP32 accumulate */
@@ -61,45 +69,59 @@ KS_API int ks_template_energy(const float* U, int64_t K, int64_t P, int64_t C,
 
 /*
  * Score matrix B[k, tau] = sum_{p,c} U[k,p,c] * sum_t W[p,t] X[c, tau - nt/2 + t]
- * (zero padding), written with leading dimension ldb >= L.
+ * (zero padding), written in b_layout (row-major with ldb >= L, or tiled).
  * Replaces kilosort/template_matching.py:180-181 (conv1d + einsum).
  */
 KS_API size_t ks_project_workspace_size(int64_t C, int64_t L, int64_t K, int64_t P,
                                  int precision);
 KS_API int ks_project(const float* X, const float* U, const float* W,
                int64_t C, int64_t L, int64_t K, int64_t P, int64_t nt,
-               int precision, float* B, int64_t ldb,
+               int precision, float* B, int64_t ldb, int b_layout,
                void* workspace, size_t workspace_bytes, void* stream);
 
 /*
- * Greedy peel on a score matrix (B [K, ldb], modified in place) and a residual
+ * Greedy peel on a score matrix (B in b_layout, modified in place) and a residual
  * (Xres [C, L], modified in place): up to max_peels iterations of detect /
  * record / subtract.  Outputs st [capacity, 2] int64 (tau, template),
  * amps [capacity], th_amps [capacity] float32, in the reference's order
- * (iteration, then tau).  th2 = Th_learned^2 rounded to float32.
+ * (iteration, then tau).  th2 = Th_learned^2 rounded to float32.  ctc is in
+ * the layout ctc_layout names; with KS_CTC_JKL a transposed copy is made in
+ * the workspace on every call, and a row-major B is tiled into the workspace
+ * and written back at the end.
  * Replaces kilosort/template_matching.py:183-244.
  */
-KS_API size_t ks_peel_workspace_size(int64_t L, int64_t K);
-KS_API int ks_peel(float* B, int64_t ldb, float* Xres, const float* U, const float* W,
-            const float* ctc, const float* nm,
+KS_API size_t ks_peel_workspace_size(int64_t L, int64_t K, int64_t nt, int b_layout,
+                                     int ctc_layout);
+KS_API int ks_peel(float* B, int64_t ldb, int b_layout, float* Xres, const float* U, const float* W,
+            const float* ctc, int ctc_layout, const float* nm,
             int64_t C, int64_t L, int64_t K, int64_t P, int64_t nt,
             float th2, int64_t max_peels, int64_t capacity,
             int64_t* st, float* amps, float* th_amps, int64_t* info,
             void* workspace, size_t workspace_bytes, void* stream);
 
 /*
- * Whole per-batch matching: Xres <- X, nm, scores, peel.
+ * Whole per-batch matching: Xres <- X, nm, scores, peel.  Callers that match
+ * many batches with one ctc pass it transposed once (KS_CTC_KJL).
  * Replaces kilosort/template_matching.py:170-244 (run_matching).
  */
 KS_API size_t ks_run_matching_workspace_size(int64_t C, int64_t L, int64_t K,
-                                      int64_t P, int precision);
+                                      int64_t P, int64_t nt, int precision,
+                                      int ctc_layout);
 KS_API int ks_run_matching(const float* X, const float* U, const float* W,
-                    const float* ctc, int64_t C, int64_t L, int64_t K,
-                    int64_t P, int64_t nt, float th2, int64_t max_peels,
-                    int precision, int64_t capacity,
+                    const float* ctc, int ctc_layout, int64_t C, int64_t L,
+                    int64_t K, int64_t P, int64_t nt, float th2,
+                    int64_t max_peels, int precision, int64_t capacity,
                     int64_t* st, float* amps, float* th_amps, float* Xres,
                     int64_t* info, void* workspace, size_t workspace_bytes,
                     void* stream);
+
+/*
+ * ctcT[k][j][lag] = ctc[j][k][lag] (not in place).  The layout the peel
+ * streams: a peak of template k subtracts one contiguous slab.
+ * Helper of kilosort/template_matching.py:238 (reads ctc[:, k, :]).
+ */
+KS_API int ks_ctc_transpose(const float* ctc, int64_t K, int64_t nt, float* ctcT,
+                            void* stream);
 
 /*
  * Per-spike PC features: tF[s, i, p] = sum_t Xres[iCC[i, iU[k_s]], tau_s - nt/2 + t]

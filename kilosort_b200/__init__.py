@@ -14,6 +14,7 @@ from .template_matching import (  # noqa: F401
     set_default_projection,
     spike_features,
     template_energy,
+    transpose_ctc,
 )
 
 __version__ = "0.1.0"

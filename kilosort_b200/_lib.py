@@ -27,6 +27,12 @@ KS_ERR_DEGENERATE = 7
 KS_PROJ_FP32 = 0
 KS_PROJ_BF16X3 = 1
 
+KS_CTC_JKL = 0
+KS_CTC_KJL = 1
+
+KS_B_ROWS = 0
+KS_B_TILED = 1
+
 _i64, _f32, _int, _sz, _vp = C.c_int64, C.c_float, C.c_int, C.c_size_t, C.c_void_p
 
 # name -> (restype, argtypes); pointers are passed as integers (c_void_p)
@@ -37,14 +43,15 @@ SIGNATURES = {
     "ks_template_energy": (_int, [_vp, _i64, _i64, _i64, _vp, _vp]),
     "ks_project_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _int]),
     "ks_project": (_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _vp,
-                          _i64, _vp, _sz, _vp]),
-    "ks_peel_workspace_size": (_sz, [_i64, _i64]),
-    "ks_peel": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64,
+                          _i64, _int, _vp, _sz, _vp]),
+    "ks_peel_workspace_size": (_sz, [_i64, _i64, _i64, _int, _int]),
+    "ks_peel": (_int, [_vp, _i64, _int, _vp, _vp, _vp, _vp, _int, _vp, _i64, _i64, _i64, _i64,
                        _i64, _f32, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
-    "ks_run_matching_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _int]),
-    "ks_run_matching": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
+    "ks_run_matching_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _i64, _int, _int]),
+    "ks_run_matching": (_int, [_vp, _vp, _vp, _vp, _int, _i64, _i64, _i64, _i64, _i64,
                                _f32, _i64, _int, _i64, _vp, _vp, _vp, _vp, _vp,
                                _vp, _sz, _vp]),
+    "ks_ctc_transpose": (_int, [_vp, _i64, _i64, _vp, _vp]),
     "ks_features": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64,
                            _i64, _i64, _i64, _i64, _vp, _vp]),
     "ks_template_channels": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp]),

@@ -63,24 +63,49 @@ int launch_template_channels(const float* U, const int64_t* iCC, int64_t K,
                              int64_t P, int64_t C, int64_t nC, int64_t* iU,
                              float* Ucc, cudaStream_t stream);
 
-// Layout of the run_matching workspace: nm, B, projection scratch, peel scratch.
+// Workspace of run_matching: nm, tiled B, projection scratch, transposed ctc
+// (only when ctc arrives in the reference layout), peel scratch.
 struct MatchLayout {
-  int64_t ldb;
-  size_t nm_off, b_off, proj_off, peel_off, bytes;
+  size_t nm_off, b_off, proj_off, ctc_off, peel_off, bytes;
 };
 
-static MatchLayout match_layout(int64_t C, int64_t L, int64_t K, int64_t P, int precision) {
+static size_t ctcT_bytes(int64_t K, int64_t nt, int ctc_layout) {
+  return ctc_layout == KS_CTC_KJL ? 0 : align256(sizeof(float) * (size_t)K * K * (2 * nt + 1));
+}
+
+static MatchLayout match_layout(int64_t C, int64_t L, int64_t K, int64_t P, int64_t nt,
+                                int precision, int ctc_layout) {
   MatchLayout m;
-  m.ldb = round_up(L, 64);
   size_t off = 0;
   m.nm_off = off;
   off = align256(off + sizeof(float) * K);
   m.b_off = off;
-  off = align256(off + sizeof(float) * (size_t)K * m.ldb);
+  off = align256(off + sizeof(float) * (size_t)tiled_rows_floats(L, K));
   m.proj_off = off;
   off = align256(off + proj_layout(C, L, K, P, precision).bytes);
+  m.ctc_off = off;
+  off += ctcT_bytes(K, nt, ctc_layout);
   m.peel_off = off;
-  off = align256(off + peel_workspace_size(L));
+  off = align256(off + peel_scratch_size(L));
+  m.bytes = off;
+  return m;
+}
+
+// Workspace of the standalone peel: tiled copy of B, transposed ctc, scratch.
+struct PeelWsLayout {
+  size_t b_off, ctc_off, peel_off, bytes;
+};
+
+static PeelWsLayout peel_ws_layout(int64_t L, int64_t K, int64_t nt, int b_layout,
+                                   int ctc_layout) {
+  PeelWsLayout m;
+  size_t off = 0;
+  m.b_off = off;
+  if (b_layout != KS_B_TILED) off = align256(off + sizeof(float) * (size_t)tiled_rows_floats(L, K));
+  m.ctc_off = off;
+  off += ctcT_bytes(K, nt, ctc_layout);
+  m.peel_off = off;
+  off = align256(off + peel_scratch_size(L));
   m.bytes = off;
   return m;
 }
@@ -135,48 +160,78 @@ size_t ks_project_workspace_size(int64_t C, int64_t L, int64_t K, int64_t P,
 
 int ks_project(const float* X, const float* U, const float* W, int64_t C,
                int64_t L, int64_t K, int64_t P, int64_t nt, int precision,
-               float* B, int64_t ldb, void* workspace, size_t workspace_bytes,
-               void* stream) {
+               float* B, int64_t ldb, int b_layout, void* workspace,
+               size_t workspace_bytes, void* stream) {
   if (!X || !U || !W || !B) return fail(KS_ERR_ARG, "ks_project: null pointer");
+  if (b_layout != KS_B_ROWS && b_layout != KS_B_TILED)
+    return fail(KS_ERR_ARG, "ks_project: unknown B layout");
   DeviceInfo d;
   int rc = device_info(&d);
   if (rc) return rc;
-  return launch_project(X, U, W, C, L, K, P, nt, precision, B, ldb, workspace,
-                        workspace_bytes, static_cast<cudaStream_t>(stream));
+  return launch_project(X, U, W, C, L, K, P, nt, precision, B, ldb, b_layout == KS_B_TILED,
+                        workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
 }
 
-size_t ks_peel_workspace_size(int64_t L, int64_t K) {
-  (void)K;
-  return peel_workspace_size(L);
+size_t ks_peel_workspace_size(int64_t L, int64_t K, int64_t nt, int b_layout,
+                              int ctc_layout) {
+  return peel_ws_layout(L, K, nt, b_layout, ctc_layout).bytes;
 }
 
-int ks_peel(float* B, int64_t ldb, float* Xres, const float* U, const float* W,
-            const float* ctc, const float* nm, int64_t C, int64_t L, int64_t K,
-            int64_t P, int64_t nt, float th2, int64_t max_peels, int64_t capacity,
-            int64_t* st, float* amps, float* th_amps, int64_t* info,
+int ks_peel(float* B, int64_t ldb, int b_layout, float* Xres, const float* U, const float* W,
+            const float* ctc, int ctc_layout, const float* nm, int64_t C, int64_t L,
+            int64_t K, int64_t P, int64_t nt, float th2, int64_t max_peels,
+            int64_t capacity, int64_t* st, float* amps, float* th_amps, int64_t* info,
             void* workspace, size_t workspace_bytes, void* stream) {
-  return launch_peel(B, ldb, Xres, U, W, ctc, nm, C, L, K, P, nt, th2, max_peels,
-                     capacity, st, amps, th_amps, info, workspace, workspace_bytes,
-                     static_cast<cudaStream_t>(stream), wait_limit_ns());
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (!B || !ctc) return fail(KS_ERR_ARG, "ks_peel: null pointer");
+  if (ctc_layout != KS_CTC_JKL && ctc_layout != KS_CTC_KJL)
+    return fail(KS_ERR_ARG, "ks_peel: unknown ctc layout");
+  if (b_layout != KS_B_ROWS && b_layout != KS_B_TILED)
+    return fail(KS_ERR_ARG, "ks_peel: unknown B layout");
+  if (K < 1 || L < 1 || nt < 1) return fail(KS_ERR_ARG, "ks_peel: bad sizes");
+  if (b_layout == KS_B_ROWS && ldb < L) return fail(KS_ERR_ARG, "ks_peel: ldb < L");
+  const PeelWsLayout m = peel_ws_layout(L, K, nt, b_layout, ctc_layout);
+  if (!workspace || workspace_bytes < m.bytes)
+    return fail(KS_ERR_WORKSPACE, "ks_peel: workspace too small");
+  char* base = static_cast<char*>(workspace);
+  float* Bt = b_layout == KS_B_TILED ? B : reinterpret_cast<float*>(base + m.b_off);
+  const float* ctcT = ctc;
+  int rc;
+  if (ctc_layout == KS_CTC_JKL) {
+    float* t = reinterpret_cast<float*>(base + m.ctc_off);
+    rc = launch_ctc_transpose(ctc, K, nt, t, s);
+    if (rc) return rc;
+    ctcT = t;
+  }
+  if (b_layout == KS_B_ROWS) {
+    rc = launch_tile_rows(B, ldb, K, L, Bt, s);
+    if (rc) return rc;
+  }
+  rc = launch_peel_tiled(Bt, Xres, U, W, ctcT, nm, C, L, K, P, nt, th2, max_peels, capacity,
+                         st, amps, th_amps, info, base + m.peel_off, m.bytes - m.peel_off, s,
+                         wait_limit_ns());
+  if (rc) return rc;
+  return b_layout == KS_B_ROWS ? launch_untile_rows(Bt, K, L, B, ldb, s) : KS_OK;
 }
 
 size_t ks_run_matching_workspace_size(int64_t C, int64_t L, int64_t K, int64_t P,
-                                      int precision) {
-  return match_layout(C, L, K, P, precision).bytes;
+                                      int64_t nt, int precision, int ctc_layout) {
+  return match_layout(C, L, K, P, nt, precision, ctc_layout).bytes;
 }
 
-int ks_run_matching(const float* X, const float* U, const float* W,
-                    const float* ctc, int64_t C, int64_t L, int64_t K, int64_t P,
-                    int64_t nt, float th2, int64_t max_peels, int precision,
-                    int64_t capacity, int64_t* st, float* amps, float* th_amps,
-                    float* Xres, int64_t* info, void* workspace,
-                    size_t workspace_bytes, void* stream) {
+int ks_run_matching(const float* X, const float* U, const float* W, const float* ctc,
+                    int ctc_layout, int64_t C, int64_t L, int64_t K, int64_t P, int64_t nt,
+                    float th2, int64_t max_peels, int precision, int64_t capacity,
+                    int64_t* st, float* amps, float* th_amps, float* Xres, int64_t* info,
+                    void* workspace, size_t workspace_bytes, void* stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (!X || !Xres) return fail(KS_ERR_ARG, "ks_run_matching: null pointer");
-  if (C < 1 || L < 1 || K < 1 || P < 1) return fail(KS_ERR_ARG, "ks_run_matching: bad sizes");
+  if (!X || !Xres || !ctc) return fail(KS_ERR_ARG, "ks_run_matching: null pointer");
+  if (C < 1 || L < 1 || K < 1 || P < 1 || nt < 1) return fail(KS_ERR_ARG, "ks_run_matching: bad sizes");
   if (precision != KS_PROJ_FP32 && precision != KS_PROJ_BF16X3)
     return fail(KS_ERR_ARG, "ks_run_matching: unknown precision");
-  const MatchLayout m = match_layout(C, L, K, P, precision);
+  if (ctc_layout != KS_CTC_JKL && ctc_layout != KS_CTC_KJL)
+    return fail(KS_ERR_ARG, "ks_run_matching: unknown ctc layout");
+  const MatchLayout m = match_layout(C, L, K, P, nt, precision, ctc_layout);
   if (!workspace || workspace_bytes < m.bytes)
     return fail(KS_ERR_WORKSPACE, "ks_run_matching: workspace too small");
   DeviceInfo d;
@@ -184,17 +239,28 @@ int ks_run_matching(const float* X, const float* U, const float* W,
   if (rc) return rc;
   char* base = static_cast<char*>(workspace);
   float* nm = reinterpret_cast<float*>(base + m.nm_off);
-  float* B = reinterpret_cast<float*>(base + m.b_off);
+  float* Bt = reinterpret_cast<float*>(base + m.b_off);
+  const float* ctcT = ctc;
+  if (ctc_layout == KS_CTC_JKL) {
+    float* t = reinterpret_cast<float*>(base + m.ctc_off);
+    rc = launch_ctc_transpose(ctc, K, nt, t, s);
+    if (rc) return rc;
+    ctcT = t;
+  }
   if (Xres != X)
     KS_CUDA(cudaMemcpyAsync(Xres, X, sizeof(float) * C * L, cudaMemcpyDeviceToDevice, s));
   rc = launch_template_energy(U, K, P, C, nm, s);
   if (rc) return rc;
-  rc = launch_project(X, U, W, C, L, K, P, nt, precision, B, m.ldb, base + m.proj_off,
-                      m.peel_off - m.proj_off, s);
+  rc = launch_project(X, U, W, C, L, K, P, nt, precision, Bt, 0, true, base + m.proj_off,
+                      m.ctc_off - m.proj_off, s);
   if (rc) return rc;
-  return launch_peel(B, m.ldb, Xres, U, W, ctc, nm, C, L, K, P, nt, th2, max_peels,
-                     capacity, st, amps, th_amps, info, base + m.peel_off,
-                     m.bytes - m.peel_off, s, wait_limit_ns());
+  return launch_peel_tiled(Bt, Xres, U, W, ctcT, nm, C, L, K, P, nt, th2, max_peels,
+                           capacity, st, amps, th_amps, info, base + m.peel_off,
+                           m.bytes - m.peel_off, s, wait_limit_ns());
+}
+
+int ks_ctc_transpose(const float* ctc, int64_t K, int64_t nt, float* ctcT, void* stream) {
+  return launch_ctc_transpose(ctc, K, nt, ctcT, static_cast<cudaStream_t>(stream));
 }
 
 int ks_features(const float* Xres, const int64_t* st, const float* amps,

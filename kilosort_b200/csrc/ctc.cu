@@ -93,7 +93,7 @@ int launch_ctc(const float* U, const float* W, int64_t K, int64_t P, int64_t C,
   const int nw = (int)(P * P * (2 * nt + 1));
   ks_wtw_kernel<<<(nw + 255) / 256, 256, 0, stream>>>(W, (int)P, (int)nt, WtW);
   KS_CUDA(cudaGetLastError());
-  int rc = sgemm_tn(Upad, Upad, G, K * P, K * P, lay.cols, lay.ldg, stream);
+  int rc = sgemm_tn(Upad, Upad, G, K * P, K * P, lay.cols, lay.ldg, stream, false);
   if (rc) return rc;
   const size_t smem = sizeof(float) * (P * P * (2 * nt + 1) + kCtcJ * P * P);
   KS_CUDA(cudaFuncSetAttribute(ks_ctc_lag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -2,51 +2,60 @@
 // cooperative kernel.  Semantics follow kilosort/template_matching.py:183-244.
 //
 // Layout in HBM
-//   B      [K, ldb]  float32 score matrix, updated in place
-//   Xres   [C, L]    float32 residual, updated in place
-//   ctc    [K, K, 2nt+1] float32, read as ctc[j, k_spike, lag]
-//   cfmax  [L] f32 / imax [L] i32   best score relu(B)^2/nm over templates and
-//                                   its template, per column (settled values)
-//   pack   [2][L] u64               per-iteration rescoring of dirty columns:
-//                                   (score bits << 32) | ~template, combined
-//                                   with atomicMax so that the larger score and,
-//                                   on ties, the smaller template index win
-//   chunk buffers                   peaks found per 512-column chunk
-//   tcount/touch/dlist [2][...]     per-iteration dirty 32-column blocks and
-//                                   the peaks touching each of them
+//   Bt     [nblk][K][32] f32   score matrix B[k, tau] tiled by 32-column blocks
+//                              (nblk = ceil(L/32)): a block's K rows are one
+//                              contiguous 128*K-byte run, so rescoring a block
+//                              streams it instead of touching K scattered lines
+//   ctcT   [K][K][2nt+1] f32   ctcT[k][j][l] = ctc[j][k][l]: the cross-
+//                              correlations a peak of template k subtracts are
+//                              one contiguous slab
+//   Xres   [C][L] f32          residual, updated in place
+//   cfmax [L] f32 / imax [L] i32  settled best score relu(B)^2/nm over
+//                              templates, and its template, per column
+//   pack   [2][L] u64          rescoring of dirty columns per iteration:
+//                              (score bits << 32) | ~template under atomicMax,
+//                              so the larger score and, on ties, the smaller
+//                              template index win
+//   per-iteration (double buffered by parity): dirty-block bitmap, touch
+//   lists (peaks within +-nt of each dirty block) and a work counter
 //
 // Iteration it (p = it & 1, q = p ^ 1), two phases between device-wide barriers:
-//   DETECT  per chunk whose +-nt neighbourhood changed in iteration it-1:
-//           settle the rescored columns (pack[q] -> cfmax/imax), then
-//           pooled = max of cfmax over +-nt; a column is a peak iff pooled > th2
-//           and |pooled - cfmax| < 1e-9 (kilosort :206-212).  Peaks are
-//           compacted in time order; amplitude B[k,tau]/nm[k] and sqrt(pooled)
-//           come from the pre-subtraction B (:225-229).  Each peak registers in
-//           the touch list of the 32-column blocks within +-nt of it; the first
-//           registration of a block appends it to dlist[p] and clears pack[p].
-//   UPDATE  every block computes the exclusive prefix of the chunk counts (the
-//           peak's global index in the iteration).  Records are written in
-//           (iteration, tau) order.  Work items (dirty block, 128-row group):
-//           for every column apply B[j,c] -= amp*ctc[j,k,c-tau+nt] of the peaks
-//           touching it, even-indexed peaks first, then odd-indexed ones -- the
-//           order of the reference's two interleaved groups (:235-238) -- with
-//           separately rounded product and difference, then fold the rescored
-//           rows into pack[p] with atomicMax.  Residual windows of every peak
-//           are updated in place (:237).
+//   DETECT  per 256-column chunk whose +-nt neighbourhood changed in it-1:
+//           settle the rescored columns (pack[q] -> cfmax/imax); pooled =
+//           max of cfmax over +-nt (doubling levels of a sliding max); a column
+//           is a peak iff pooled > th2 and |pooled - cfmax| < 1e-9 (kilosort
+//           :206-212).  Peaks are compacted in time order; amplitude
+//           B[k,tau]/nm[k] and sqrt(pooled) come from the pre-subtraction B
+//           (:225-229).  Each peak registers in the touch lists of the blocks
+//           within +-nt of it; the first registration sets the block's dirty bit
+//           and clears its pack[p] entries.
+//   UPDATE  every block computes the exclusive prefix of the chunk counts (a
+//           peak's global index in the iteration) and of the dirty bitmap.
+//           Records are written in (iteration, tau) order.  Warps take work
+//           items from a counter: (dirty block in column order, row range):
+//           B[j,c] -= amp*ctc[j,k,c-tau+nt] for the peaks touching column c,
+//           even-indexed peaks first, then odd-indexed -- the order of the
+//           reference's two interleaved groups (:235-238) -- product and
+//           difference rounded separately; rescored rows fold into pack[p].
+//           Then (peak, 8 channels) items update the residual windows (:237).
 // The loop ends when no peak is found or after max_peels iterations, decided
 // identically by every block from the same counts.  Every device-wide wait is
 // bounded; a wait that runs out records KS_ERR_TIMEOUT and all blocks leave.
 #include "ks_common.cuh"
+#include "project.cuh"
 
 namespace {
 
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
-constexpr int kChunk = 512;          // detection chunk, one column per thread
+constexpr int kChunk = 256;          // detection chunk, one column per thread
 constexpr int kCol = 32;             // update block, one column per lane
 constexpr int kRowsPerWarp = 8;      // template rows in flight per lane
+constexpr int kItemRows = 64;        // template rows per update item (at most)
 constexpr int kTouch = 8;            // peaks touching one block (more: ties)
-constexpr int kMaxChunks = 8192;
+constexpr int kXresChans = 8;        // channels per residual item
+constexpr int kGrab = 2;             // work items taken per counter increment
+constexpr int kMaxChunks = 16384;
 
 // Phase timeline for profiling builds (-DKS_PEEL_TRACE): block 0 writes
 // %globaltimer stamps to info[8 + 8*it + slot]; the caller sizes info.
@@ -70,12 +79,11 @@ struct Touch {
 };
 
 struct PeelArgs {
-  float* B;
-  long long ldb;
+  float* Bt;
   float* Xres;
   const float* U;
   const float* W;
-  const float* ctc;
+  const float* ctcT;
   const float* nm;
   int C, L, K, P, nt;
   float th2;
@@ -96,17 +104,18 @@ struct PeelArgs {
   float* chunk_th;
   int* tcount;                // [2][nblk]
   Touch* touch;               // [2][nblk * kTouch]
-  int* dlist;                 // [2][nblk]
-  int* dcount;                // [2]
+  unsigned* dbits;            // [2][nwords]
+  unsigned* wctr;             // [2] work counters
   unsigned* bar;              // {count, generation}
   int* err;
-  int nchunks, nblk;
+  int nchunks, nblk, nwords;
   unsigned long long limit_ns;
 };
 
 struct Smem {
   float* W;        // P*nt
-  int* prefix;     // nchunks+1
+  int* prefix;     // nchunks+1   exclusive prefix of chunk peak counts
+  int* wprefix;    // nwords+1    exclusive prefix of dirty-bitmap popcounts
   float* win;      // kChunk + 2*nt   column scores around the chunk
   float* mx0;      // kChunk + 2*nt   sliding-max doubling levels (ping-pong)
   float* mx1;      // kChunk + 2*nt
@@ -129,6 +138,7 @@ __device__ __forceinline__ Smem carve_smem(const PeelArgs& a, char* base) {
   const int wn = kChunk + 2 * a.nt;
   s.W = reinterpret_cast<float*>(take(sizeof(float) * a.P * a.nt));
   s.prefix = reinterpret_cast<int*>(take(sizeof(int) * (a.nchunks + 1)));
+  s.wprefix = reinterpret_cast<int*>(take(sizeof(int) * (a.nwords + 1)));
   s.win = reinterpret_cast<float*>(take(sizeof(float) * wn));
   s.mx0 = reinterpret_cast<float*>(take(sizeof(float) * wn));
   s.mx1 = reinterpret_cast<float*>(take(sizeof(float) * wn));
@@ -141,11 +151,12 @@ __device__ __forceinline__ Smem carve_smem(const PeelArgs& a, char* base) {
   return s;
 }
 
-size_t smem_bytes(int P, int nt, int nchunks) {
+size_t smem_bytes(int P, int nt, int nchunks, int nwords) {
   auto r = [](size_t b) { return (b + 15) & ~size_t(15); };
   const size_t wn = kChunk + 2 * (size_t)nt;
   return r(sizeof(float) * P * nt) + r(sizeof(int) * (nchunks + 1)) +
-         3 * r(sizeof(float) * wn) + r(sizeof(int) * kChunk) + r(sizeof(int) * (kWarps + 1)) +
+         r(sizeof(int) * (nwords + 1)) + 3 * r(sizeof(float) * wn) +
+         r(sizeof(int) * kChunk) + r(sizeof(int) * (kWarps + 1)) +
          3 * r(sizeof(int) * kWarps * kTouch) + r(sizeof(float) * kWarps * 64);
 }
 
@@ -157,6 +168,9 @@ __device__ __forceinline__ float pack_value(unsigned long long v) {
 }
 __device__ __forceinline__ int pack_index(unsigned long long v) {
   return (int)(~(unsigned)(v & 0xffffffffull));
+}
+__device__ __forceinline__ const float* bt_row(const PeelArgs& a, int blk, int j) {
+  return a.Bt + ((size_t)blk * a.K + j) * kCol;
 }
 
 // ---------------------------------------------------------------- DETECT
@@ -224,7 +238,7 @@ __device__ void detect_chunk(const PeelArgs& a, const Smem& s, int ch, int it) {
   const int tau = a0 + tid;
   bool pk = false;
   float pooled = 0.f;
-  if (tau < a1 && tau >= nt && tau < L - nt) {
+  if (tid < kChunk && tau < a1 && tau >= nt && tau < L - nt) {
     pooled = fmaxf(src[tid], src[tid + len - m]);
     const float best = s.win[tid + nt];
     pk = (pooled > a.th2) && (fabsf(__fsub_rn(pooled, best)) < 1e-9f);
@@ -245,7 +259,7 @@ __device__ void detect_chunk(const PeelArgs& a, const Smem& s, int ch, int it) {
   if (pk) {
     const int idx = s.wcnt[warp] + __popc(bal & ((1u << lane) - 1u));
     const int k = s.kidx[tid];
-    const float amp = __fdiv_rn(a.B[(long long)k * a.ldb + tau], a.nm[k]);
+    const float amp = __fdiv_rn(bt_row(a, tau / kCol, k)[tau % kCol], a.nm[k]);
     const float th = __fsqrt_rn(pooled);
     const int slot = ch * kChunk + idx;
     a.chunk_tau[slot] = tau;
@@ -254,6 +268,7 @@ __device__ void detect_chunk(const PeelArgs& a, const Smem& s, int ch, int it) {
     a.chunk_th[slot] = th;
     int* tcur = a.tcount + (size_t)p * a.nblk;
     Touch* tch = a.touch + (size_t)p * a.nblk * kTouch;
+    unsigned* bits = a.dbits + (size_t)p * a.nwords;
     unsigned long long* pcur = a.pack + (size_t)p * L;
     const int b0 = (tau - nt) / kCol, b1 = (tau + nt) / kCol;
     for (int bb = b0; bb <= b1; bb += 8) {
@@ -265,8 +280,7 @@ __device__ void detect_chunk(const PeelArgs& a, const Smem& s, int ch, int it) {
         const int b = bb + i;
         if (pos[i] < 0) continue;
         if (pos[i] == 0) {
-          const int d = atomicAdd(&a.dcount[p], 1);
-          a.dlist[(size_t)p * a.nblk + d] = b;
+          atomicOr(&bits[b >> 5], 1u << (b & 31));
           const int c_hi = min(L, (b + 1) * kCol);
           for (int c = b * kCol; c < c_hi; ++c) pcur[c] = 0ull;
         }
@@ -279,53 +293,52 @@ __device__ void detect_chunk(const PeelArgs& a, const Smem& s, int ch, int it) {
   __syncthreads();
 }
 
-// Exclusive prefix of chunk counts into s.prefix[0..nchunks]; returns total.
-__device__ int chunk_prefix(const PeelArgs& a, const Smem& s) {
+// Exclusive prefix of n counts (read through get(i)) into out[0..n]; returns
+// the total.  All threads of the block take part.
+template <typename Get>
+__device__ int block_prefix(int n, Get get, int* out, int* wcnt) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int per = (a.nchunks + kThreads - 1) / kThreads;
+  const int per = (n + kThreads - 1) / kThreads;
   const int c0 = tid * per;
   int local = 0;
   for (int i = 0; i < per; ++i) {
     const int c = c0 + i;
-    if (c < a.nchunks) local += a.chunk_cnt[c];
+    if (c < n) local += get(c);
   }
   int incl = local;
   for (int o = 1; o < 32; o <<= 1) {
     const int v = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += v;
   }
-  if (lane == 31) s.wcnt[warp] = incl;
+  if (lane == 31) wcnt[warp] = incl;
   __syncthreads();
   if (tid == 0) {
     int acc = 0;
     for (int w = 0; w < kWarps; ++w) {
-      const int c = s.wcnt[w];
-      s.wcnt[w] = acc;
+      const int c = wcnt[w];
+      wcnt[w] = acc;
       acc += c;
     }
-    s.wcnt[kWarps] = acc;
+    wcnt[kWarps] = acc;
   }
   __syncthreads();
-  int run = s.wcnt[warp] + incl - local;
+  int run = wcnt[warp] + incl - local;
   for (int i = 0; i < per; ++i) {
     const int c = c0 + i;
-    if (c < a.nchunks) {
-      s.prefix[c] = run;
-      run += a.chunk_cnt[c];
+    if (c < n) {
+      out[c] = run;
+      run += get(c);
     }
   }
-  if (tid == 0) s.prefix[a.nchunks] = s.wcnt[kWarps];
+  if (tid == 0) out[n] = wcnt[kWarps];
   __syncthreads();
-  return s.prefix[a.nchunks];
+  return out[n];
 }
 
 // ---------------------------------------------------------------- UPDATE
-// Work items are per warp (no block-wide synchronisation), so thousands run
-// concurrently and the latency of one item hides behind the others.
-
-// Ordered touch list of one 32-column block in the warp's shared-memory
-// slot: entry e (application order: even global index first, then odd, each
-// ascending) has peak time tau[e], template k[e], amplitude amp[e].
+// Ordered touch list of one block in the warp's shared-memory slot: entry e
+// (application order: even global index first, then odd, each ascending) has
+// peak time tau[e], template k[e], amplitude amp[e].
 struct TouchList {
   int n;
   const int* tau;
@@ -363,17 +376,16 @@ __device__ __forceinline__ TouchList load_touch_warp(const PeelArgs& a, const Sm
   return TouchList{n, tau, kk, amp};
 }
 
-// Columns [blk*32, blk*32+32) x template rows [j_lo, j_hi): subtract the
-// touching peaks, store the changed rows, fold the rescored rows into pack_out.
-// A column is touched by at most two peaks unless scores tie exactly; the two
-// are preloaded with the rows of B so each group of rows costs one round trip.
+// Columns of block blk x template rows [j_lo, j_hi): subtract the touching
+// peaks, store the changed rows, fold the rescored rows into pack_out.  A
+// column is touched by at most two peaks unless scores tie exactly; those two
+// are loaded with the rows of B so a group of rows costs one round trip.
 __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk,
                                  int j_lo, int j_hi, unsigned long long* pack_out,
                                  int lane) {
   const int c = blk * kCol + lane;
   const bool colok = c < a.L;
   const int nt = a.nt, K = a.K, nlag = 2 * nt + 1;
-  const long long rstride = (long long)K * nlag;     // ctc row stride (j)
   int e0 = -1, e1 = -1;
   unsigned rest = 0u;                                 // further touching entries
   for (int e = 0; e < tl.n; ++e) {
@@ -385,11 +397,12 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
     }
   }
   const bool touched = e0 >= 0;
-  const float* cp0 = a.ctc;
-  const float* cp1 = a.ctc;
+  const float* cp0 = a.ctcT;
+  const float* cp1 = a.ctcT;
   float amp0 = 0.f, amp1 = 0.f;
-  if (e0 >= 0) { cp0 = a.ctc + (long long)tl.k[e0] * nlag + (c - tl.tau[e0] + nt); amp0 = tl.amp[e0]; }
-  if (e1 >= 0) { cp1 = a.ctc + (long long)tl.k[e1] * nlag + (c - tl.tau[e1] + nt); amp1 = tl.amp[e1]; }
+  if (e0 >= 0) { cp0 = a.ctcT + (size_t)tl.k[e0] * K * nlag + (c - tl.tau[e0] + nt); amp0 = tl.amp[e0]; }
+  if (e1 >= 0) { cp1 = a.ctcT + (size_t)tl.k[e1] * K * nlag + (c - tl.tau[e1] + nt); amp1 = tl.amp[e1]; }
+  float* bcol = a.Bt + (size_t)blk * K * kCol + lane;
   float best = -1.f;
   int arg = 0;
   for (int j0 = j_lo; j0 < j_hi; j0 += kRowsPerWarp) {
@@ -398,9 +411,9 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
     for (int r = 0; r < kRowsPerWarp; ++r) {
       const int j = j0 + r;
       const bool ok = colok && j < j_hi;
-      bv[r] = ok ? a.B[(long long)j * a.ldb + c] : 0.f;
-      w0[r] = (ok && e0 >= 0) ? __ldg(cp0 + j * rstride) : 0.f;
-      w1[r] = (ok && e1 >= 0) ? __ldg(cp1 + j * rstride) : 0.f;
+      bv[r] = ok ? bcol[(size_t)j * kCol] : 0.f;
+      w0[r] = (ok && e0 >= 0) ? __ldg(cp0 + (size_t)j * nlag) : 0.f;
+      w1[r] = (ok && e1 >= 0) ? __ldg(cp1 + (size_t)j * nlag) : 0.f;
     }
 #pragma unroll
     for (int r = 0; r < kRowsPerWarp; ++r) {
@@ -411,11 +424,11 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
       for (int e = 0; e < tl.n; ++e) {
         if ((rest >> e) & 1u) {
           const float amp = tl.amp[e];
-          const float* cp = a.ctc + (long long)tl.k[e] * nlag + (c - tl.tau[e] + nt);
+          const float* cp = a.ctcT + (size_t)tl.k[e] * K * nlag + (c - tl.tau[e] + nt);
 #pragma unroll
           for (int r = 0; r < kRowsPerWarp; ++r) {
             const int j = j0 + r;
-            if (j < j_hi) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp, __ldg(cp + j * rstride)));
+            if (j < j_hi) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp, __ldg(cp + (size_t)j * nlag)));
           }
         }
       }
@@ -424,7 +437,7 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
     for (int r = 0; r < kRowsPerWarp; ++r) {
       const int j = j0 + r;
       if (colok && j < j_hi) {
-        if (touched) a.B[(long long)j * a.ldb + c] = bv[r];
+        if (touched) bcol[(size_t)j * kCol] = bv[r];
         const float rl = bv[r] > 0.f ? bv[r] : 0.f;
         const float cf = __fdiv_rn(__fmul_rn(rl, rl), __ldg(a.nm + j));
         if (cf > best) {
@@ -440,8 +453,7 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
 // Subtract amp * sum_p U[k,p,c] W[p,t] from Xres[c, tau - nt/2 + t] for 8
 // channels of one peak; lanes run along t.  The U values of the 8 channels go
 // through the warp's shared-memory slot and all residual values of a 64-tap
-// span are loaded before any is written, so one item costs two round trips.
-constexpr int kXresChans = 8;
+// span are loaded before any is written.
 __device__ void xres_warp_item(const PeelArgs& a, const Smem& s, int sp, int cg,
                                int lane, int warp) {
   int lo = 0, hi = a.nchunks - 1;
@@ -489,26 +501,40 @@ __device__ void xres_warp_item(const PeelArgs& a, const Smem& s, int sp, int cg,
   }
 }
 
+// Block of the rank-th set bit of the dirty bitmap (s.wprefix holds the
+// exclusive prefix of the word popcounts).
+__device__ __forceinline__ int dirty_block(const Smem& s, const unsigned* bits,
+                                           int nwords, int rank) {
+  int lo = 0, hi = nwords - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (s.wprefix[mid] <= rank) lo = mid; else hi = mid - 1;
+  }
+  const unsigned word = bits[lo];
+  const int bit = (int)__fns(word, 0, rank - s.wprefix[lo] + 1);
+  return lo * 32 + bit;
+}
+
 __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   const Smem s = carve_smem(a, smem_raw);
   const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
   const unsigned G = gridDim.x;
+  const long long gwarp = (long long)blockIdx.x * kWarps + warp;
+  const long long nwarps = (long long)G * kWarps;
   for (int i = tid; i < a.P * a.nt; i += kThreads) s.W[i] = a.W[i];
   __syncthreads();
 
   // initial scores of every column, folded into pack[1] (zeroed by the host)
-  const int lane = tid & 31;
-  const long long gwarp = (long long)blockIdx.x * kWarps + (tid >> 5);
-  const long long nwarps = (long long)G * kWarps;
   {
     unsigned long long* pinit = a.pack + (size_t)a.L;
-    const int rg = (int)((a.K + 63) / 64);
+    const int rg = (a.K + kItemRows - 1) / kItemRows;
     const TouchList none{0, nullptr, nullptr, nullptr};
     const long long n_items = (long long)a.nblk * rg;
     for (long long w = gwarp; w < n_items; w += nwarps) {
       const int blk = (int)(w / rg), r = (int)(w % rg);
-      update_warp_item(a, none, blk, r * 64, min(a.K, (r + 1) * 64), pinit, lane);
+      update_warp_item(a, none, blk, r * kItemRows, min(a.K, (r + 1) * kItemRows), pinit, lane);
     }
   }
 
@@ -525,16 +551,20 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
     if (!ks_grid_sync(a.bar, G, a.err, a.limit_ns)) break;
     KS_TRACE(it, 2, ks_globaltimer());
 
-    const int total = chunk_prefix(a, s);
+    const int* cnt = a.chunk_cnt;
+    const int total = block_prefix(a.nchunks, [cnt](int i) { return cnt[i]; }, s.prefix, s.wcnt);
     if (total == 0) break;
     if (n_out + total > a.capacity) {
       status = KS_ERR_OVERFLOW;
       if (blockIdx.x == 0 && tid == 0) a.info[3] = n_out + total;
       break;
     }
+    const unsigned* bits = a.dbits + (size_t)p * a.nwords;
+    const int ndirty = block_prefix(a.nwords, [bits](int i) { return __popc(bits[i]); },
+                                    s.wprefix, s.wcnt);
     for (int ch = blockIdx.x; ch < a.nchunks; ch += G) {
-      const int cnt = a.chunk_cnt[ch];
-      for (int i = tid; i < cnt; i += kThreads) {
+      const int c_n = a.chunk_cnt[ch];
+      for (int i = tid; i < c_n; i += kThreads) {
         const long long slot = (long long)ch * kChunk + i;
         const long long o = n_out + s.prefix[ch] + i;
         a.st[2 * o] = a.chunk_tau[slot];
@@ -543,34 +573,43 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
         a.th_amps[o] = a.chunk_th[slot];
       }
     }
-    // registration lists of the next iteration start empty
+    // registration lists, bitmap and work counter of the next iteration start empty
     for (int w = blockIdx.x * kThreads + tid; w < a.nblk; w += G * kThreads)
       a.tcount[(size_t)q * a.nblk + w] = 0;
-    if (blockIdx.x == 0 && tid == 0) a.dcount[q] = 0;
-    // subtract and rescore dirty blocks; residual windows -- one work list of
-    // warp items, row ranges sized so that every warp gets about two items
-    const int ndirty = a.dcount[p];
-    int rgroups = 1;
+    for (int w = blockIdx.x * kThreads + tid; w < a.nwords; w += G * kThreads)
+      a.dbits[(size_t)q * a.nwords + w] = 0u;
+    if (blockIdx.x == 0 && tid == 0) a.wctr[q] = 0u;
+    // update items: (dirty block in column order, row range), sized so that
+    // there are about four per warp; then residual items
+    int rows = kItemRows;
     if (ndirty > 0) {
-      const long long want = (2 * nwarps + ndirty - 1) / ndirty;
-      const long long cap = (a.K + kRowsPerWarp - 1) / kRowsPerWarp;
-      rgroups = (int)(want < 1 ? 1 : (want > cap ? cap : want));
+      const long long per_blk = (4 * nwarps + ndirty - 1) / ndirty;   // items wanted per block
+      const int r = (int)((a.K + per_blk - 1) / per_blk);
+      rows = max(kRowsPerWarp, min(kItemRows, r));
     }
-    const int rows = (a.K + rgroups - 1) / rgroups;
+    const int rgroups = (a.K + rows - 1) / rows;
     const long long n_upd = (long long)ndirty * rgroups;
     const int xgroups = (a.C + kXresChans - 1) / kXresChans;
-    const long long n_x = (long long)total * xgroups;
+    const long long n_items = n_upd + (long long)total * xgroups;
     unsigned long long* pcur = a.pack + (size_t)p * a.L;
     KS_TRACE(it, 3, ks_globaltimer());
-    for (long long w = gwarp; w < n_upd + n_x; w += nwarps) {
-      if (w < n_upd) {
-        const int blk = a.dlist[(size_t)p * a.nblk + (int)(w / rgroups)];
-        const int r = (int)(w % rgroups);
-        const TouchList tl = load_touch_warp(a, s, p, blk, lane, tid >> 5);
-        update_warp_item(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
-      } else {
-        const long long x = w - n_upd;
-        xres_warp_item(a, s, (int)(x / xgroups), (int)(x % xgroups), lane, tid >> 5);
+    while (true) {
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(&a.wctr[p], (unsigned)kGrab);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if ((long long)base >= n_items) break;
+      for (int g = 0; g < kGrab; ++g) {
+        const long long w = (long long)base + g;
+        if (w >= n_items) break;
+        if (w < n_upd) {
+          const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
+          const int r = (int)(w % rgroups);
+          const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
+          update_warp_item(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
+        } else {
+          const long long x = w - n_upd;
+          xres_warp_item(a, s, (int)(x / xgroups), (int)(x % xgroups), lane, warp);
+        }
       }
     }
     KS_TRACE(it, 4, ks_globaltimer());
@@ -588,21 +627,62 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
   }
 }
 
+// ------------------------------------------------------------------ relayout
+__global__ void ks_tile_rows_kernel(const float* __restrict__ B, long long ldb, int K,
+                                    int L, int nblk, float* __restrict__ Bt) {
+  const long long n = (long long)nblk * K * kCol;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(e % kCol);
+    const long long bj = e / kCol;
+    const int j = (int)(bj % K);
+    const int blk = (int)(bj / K);
+    const int col = blk * kCol + c;
+    Bt[e] = col < L ? B[(long long)j * ldb + col] : 0.f;
+  }
+}
+
+__global__ void ks_untile_rows_kernel(const float* __restrict__ Bt, int K, int L,
+                                      float* __restrict__ B, long long ldb) {
+  const long long n = (long long)K * L;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int col = (int)(e % L);
+    const int j = (int)(e / L);
+    B[(long long)j * ldb + col] = Bt[((long long)(col / kCol) * K + j) * kCol + (col % kCol)];
+  }
+}
+
+__global__ void ks_ctc_transpose_kernel(const float* __restrict__ ctc, int K, int nlag,
+                                        float* __restrict__ ctcT) {
+  // ctcT[k][j][l] = ctc[j][k][l]; one row of nlag contiguous floats per (k, j)
+  const long long rows = (long long)K * K;
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int k = (int)(r / K), j = (int)(r % K);
+    const float* src = ctc + ((long long)j * K + k) * nlag;
+    float* dst = ctcT + r * nlag;
+    for (int l = threadIdx.x; l < nlag; l += blockDim.x) dst[l] = src[l];
+  }
+}
+
 struct PeelLayout {
-  int nchunks, nblk;
+  int nchunks, nblk, nwords;
   size_t zero_bytes;   // leading bytes that must start at zero
   size_t bytes;
 };
 
-// Workspace order: [ctl: bar(2) err(1) pad(1) dcount(2) pad(2)] [tcount 2*nblk]
-// [pack 2*L] -- the leading part up to and including pack[1] is zeroed per launch.
+// Workspace order: [ctl: bar(2) err(1) pad(1) wctr(2) pad(2)] [tcount 2*nblk]
+// [dbits 2*nwords] [pack 2*L] -- everything up to the end of pack[1] is
+// zeroed per launch -- then the settled scores, chunk buffers and touch lists.
 PeelLayout peel_layout(int64_t L) {
   PeelLayout l;
   l.nchunks = (int)((L + kChunk - 1) / kChunk);
   l.nblk = (int)((L + kCol - 1) / kCol);
+  l.nwords = (l.nblk + 31) / 32;
   ks::Carve cv(nullptr);
   cv.take<unsigned>(8);
   cv.take<int>(2 * (size_t)l.nblk);
+  cv.take<unsigned>(2 * (size_t)l.nwords);
   cv.take<unsigned long long>(2 * (size_t)L);
   l.zero_bytes = cv.used;
   cv.take<float>(L);
@@ -610,7 +690,6 @@ PeelLayout peel_layout(int64_t L) {
   cv.take<int>(l.nchunks);
   for (int i = 0; i < 4; ++i) cv.take<int>((size_t)l.nchunks * kChunk);
   cv.take<Touch>(2 * (size_t)l.nblk * kTouch);
-  cv.take<int>(2 * (size_t)l.nblk);
   l.bytes = cv.used;
   return l;
 }
@@ -619,21 +698,48 @@ PeelLayout peel_layout(int64_t L) {
 
 namespace ks {
 
-size_t peel_workspace_size(int64_t L) { return peel_layout(L).bytes; }
+size_t peel_scratch_size(int64_t L) { return peel_layout(L).bytes; }
 
-int launch_peel(float* B, int64_t ldb, float* Xres, const float* U,
-                const float* W, const float* ctc, const float* nm, int64_t C,
-                int64_t L, int64_t K, int64_t P, int64_t nt, float th2,
-                int64_t max_peels, int64_t capacity, int64_t* st, float* amps,
-                float* th_amps, int64_t* info, void* ws, size_t ws_bytes,
-                cudaStream_t stream, unsigned long long limit_ns) {
-  if (!B || !Xres || !U || !W || !ctc || !nm || !st || !amps || !th_amps || !info)
+int64_t tiled_rows_floats(int64_t L, int64_t K) { return ((L + kCol - 1) / kCol) * K * kCol; }
+
+int launch_tile_rows(const float* B, int64_t ldb, int64_t K, int64_t L, float* Bt,
+                     cudaStream_t stream) {
+  const int nblk = (int)((L + kCol - 1) / kCol);
+  ks_tile_rows_kernel<<<2048, 256, 0, stream>>>(B, ldb, (int)K, (int)L, nblk, Bt);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
+int launch_untile_rows(const float* Bt, int64_t K, int64_t L, float* B, int64_t ldb,
+                       cudaStream_t stream) {
+  ks_untile_rows_kernel<<<2048, 256, 0, stream>>>(Bt, (int)K, (int)L, B, ldb);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
+int launch_ctc_transpose(const float* ctc, int64_t K, int64_t nt, float* ctcT,
+                         cudaStream_t stream) {
+  if (!ctc || !ctcT || K < 1 || nt < 1) return fail(KS_ERR_ARG, "ks_ctc_transpose: bad args");
+  if (ctc == ctcT) return fail(KS_ERR_ARG, "ks_ctc_transpose: in-place transpose is not supported");
+  const long long rows = K * K;
+  const int grid = (int)std::min<long long>(rows, 65535LL * 4);
+  ks_ctc_transpose_kernel<<<grid, 128, 0, stream>>>(ctc, (int)K, (int)(2 * nt + 1), ctcT);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
+int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
+                      const float* ctcT, const float* nm, int64_t C, int64_t L, int64_t K,
+                      int64_t P, int64_t nt, float th2, int64_t max_peels,
+                      int64_t capacity, int64_t* st, float* amps, float* th_amps,
+                      int64_t* info, void* ws, size_t ws_bytes, cudaStream_t stream,
+                      unsigned long long limit_ns) {
+  if (!Bt || !Xres || !U || !W || !ctcT || !nm || !st || !amps || !th_amps || !info)
     return fail(KS_ERR_ARG, "ks_peel: null pointer");
   if (C < 1 || L < 1 || K < 1 || P < 1 || nt < 1 || (nt % 2) == 0)
     return fail(KS_ERR_ARG, "ks_peel: need C,L,K,P >= 1 and odd nt");
-  if (ldb < L) return fail(KS_ERR_ARG, "ks_peel: ldb < L");
-  if (L > (int64_t)kMaxChunks * kChunk || K > (1 << 24) || C > (1 << 24) ||
-      nt > 1023 || P > 8)
+  if (L > (int64_t)kMaxChunks * kChunk || K > (1 << 24) || C > (1 << 24) || nt > 1023 ||
+      P > 8)
     return fail(KS_ERR_UNSUPPORTED, "ks_peel: shape beyond supported limits");
   if (capacity < 0 || max_peels < 0) return fail(KS_ERR_ARG, "ks_peel: negative capacity/max_peels");
   if (!(th2 >= 0.f)) return fail(KS_ERR_ARG, "ks_peel: th2 must be a non-negative number");
@@ -645,7 +751,7 @@ int launch_peel(float* B, int64_t ldb, float* Xres, const float* U,
   if (rc) return rc;
 
   PeelArgs a{};
-  a.B = B; a.ldb = ldb; a.Xres = Xres; a.U = U; a.W = W; a.ctc = ctc; a.nm = nm;
+  a.Bt = Bt; a.Xres = Xres; a.U = U; a.W = W; a.ctcT = ctcT; a.nm = nm;
   a.C = (int)C; a.L = (int)L; a.K = (int)K; a.P = (int)P; a.nt = (int)nt;
   a.th2 = th2;
   a.max_peels = (int)std::min<int64_t>(max_peels, 1 << 30);
@@ -656,8 +762,9 @@ int launch_peel(float* B, int64_t ldb, float* Xres, const float* U,
   unsigned* ctl = cv.take<unsigned>(8);
   a.bar = ctl;
   a.err = reinterpret_cast<int*>(ctl + 2);
-  a.dcount = reinterpret_cast<int*>(ctl + 4);
+  a.wctr = ctl + 4;
   a.tcount = cv.take<int>(2 * (size_t)lay.nblk);
+  a.dbits = cv.take<unsigned>(2 * (size_t)lay.nwords);
   a.pack = cv.take<unsigned long long>(2 * (size_t)L);
   a.cfmax = cv.take<float>(L);
   a.imax = cv.take<int>(L);
@@ -667,17 +774,16 @@ int launch_peel(float* B, int64_t ldb, float* Xres, const float* U,
   a.chunk_amp = cv.take<float>((size_t)lay.nchunks * kChunk);
   a.chunk_th = cv.take<float>((size_t)lay.nchunks * kChunk);
   a.touch = cv.take<Touch>(2 * (size_t)lay.nblk * kTouch);
-  a.dlist = cv.take<int>(2 * (size_t)lay.nblk);
-  a.nchunks = lay.nchunks; a.nblk = lay.nblk;
+  a.nchunks = lay.nchunks; a.nblk = lay.nblk; a.nwords = lay.nwords;
   a.limit_ns = limit_ns;
 
-  const size_t smem = smem_bytes(a.P, a.nt, a.nchunks);
+  const size_t smem = smem_bytes(a.P, a.nt, a.nchunks, a.nwords);
+  if (smem > dev.smem_optin) return fail(KS_ERR_UNSUPPORTED, "ks_peel: batch too long for shared memory");
   static thread_local int cached_dev = -1;
   static thread_local size_t cached_smem = 0;
   static thread_local int cached_occ = 0;
   if (cached_dev != dev.device || cached_smem != smem) {
-    if (smem > 48 * 1024)
-      KS_CUDA(cudaFuncSetAttribute(peel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    KS_CUDA(cudaFuncSetAttribute(peel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
     KS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, peel_kernel, kThreads, smem));
     if (occ < 1) return fail(KS_ERR_UNSUPPORTED, "ks_peel: kernel does not fit on an SM");

@@ -145,7 +145,10 @@ size_t temporal_smem(int nt, int P) {
 constexpr int kBM = 128, kBN = 128, kBK = 16;
 
 // C[m, n] = sum_q A[m, q] * Bt[n, q]; A is [>= tiles_m*128, Kd], Bt is
-// [>= tiles_n*128, Kd] (both zero padded), Kd % 16 == 0.  Stores m < M, n < N.
+// [>= tiles_n*128, Kd] (both zero padded), Kd % 16 == 0.  Stores m < M, n < N,
+// row-major with leading dimension ldc, or (kTiled) in 32-column blocks
+// C[((n/32)*M + m)*32 + n%32].
+template <bool kTiled>
 __global__ void __launch_bounds__(256, 2)
 ks_sgemm_tn_kernel(const float* __restrict__ A, const float* __restrict__ Bt,
                    float* __restrict__ Cm, int M, int N, int Kd, long long ldc,
@@ -223,7 +226,7 @@ ks_sgemm_tn_kernel(const float* __restrict__ A, const float* __restrict__ Bt,
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const long long n = n0 + h * 64 + tx * 4;
-      float* dst = Cm + m * ldc + n;
+      float* dst = kTiled ? Cm + (((n >> 5) * M + m) << 5) + (n & 31) : Cm + m * ldc + n;
       const float* v = &acc[i][h * 4];
       if (n + 3 < N && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0)) {
         *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
@@ -236,14 +239,18 @@ ks_sgemm_tn_kernel(const float* __restrict__ A, const float* __restrict__ Bt,
 }
 
 int sgemm_tn(const float* A, const float* Bt, float* Cm, int64_t M, int64_t N,
-             int64_t Kd, int64_t ldc, cudaStream_t stream) {
+             int64_t Kd, int64_t ldc, cudaStream_t stream, bool tiled) {
   if (Kd % kBK) return fail(KS_ERR_ARG, "sgemm_tn: Kd must be a multiple of 16");
   const int tiles_m = (int)((M + kBM - 1) / kBM);
   const int tiles_n = (int)((N + kBN - 1) / kBN);
   const long long nblocks = (long long)tiles_m * tiles_n;
   if (nblocks > 0x7fffffffLL) return fail(KS_ERR_UNSUPPORTED, "sgemm_tn: too many tiles");
-  ks_sgemm_tn_kernel<<<(unsigned)nblocks, 256, 0, stream>>>(A, Bt, Cm, (int)M, (int)N,
-                                                            (int)Kd, ldc, tiles_m);
+  if (tiled)
+    ks_sgemm_tn_kernel<true><<<(unsigned)nblocks, 256, 0, stream>>>(A, Bt, Cm, (int)M, (int)N,
+                                                                  (int)Kd, ldc, tiles_m);
+  else
+    ks_sgemm_tn_kernel<false><<<(unsigned)nblocks, 256, 0, stream>>>(A, Bt, Cm, (int)M, (int)N,
+                                                                   (int)Kd, ldc, tiles_m);
   KS_CUDA(cudaGetLastError());
   return KS_OK;
 }
@@ -317,14 +324,14 @@ int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
 
 int launch_project(const float* X, const float* U, const float* W, int64_t C,
                    int64_t L, int64_t K, int64_t P, int64_t nt, int precision,
-                   float* B, int64_t ldb, void* ws, size_t ws_bytes,
+                   float* B, int64_t ldb, bool tiled, void* ws, size_t ws_bytes,
                    cudaStream_t stream) {
   if (!X || !U || !W || !B) return fail(KS_ERR_ARG, "ks_project: null pointer");
   if (C < 1 || L < 1 || K < 1 || P < 1 || nt < 1 || (nt % 2) == 0)
     return fail(KS_ERR_ARG, "ks_project: need C,L,K,P >= 1 and odd nt");
   if (P > kPMax) return fail(KS_ERR_UNSUPPORTED, "ks_project: n_pcs must be <= 8");
   if (nt > 1023) return fail(KS_ERR_UNSUPPORTED, "ks_project: nt must be <= 1023");
-  if (ldb < L) return fail(KS_ERR_ARG, "ks_project: ldb < L");
+  if (!tiled && ldb < L) return fail(KS_ERR_ARG, "ks_project: ldb < L");
   if (precision != KS_PROJ_FP32 && precision != KS_PROJ_BF16X3)
     return fail(KS_ERR_ARG, "ks_project: unknown precision");
   const ProjLayout lay = proj_layout(C, L, K, P, precision);
@@ -339,7 +346,7 @@ int launch_project(const float* X, const float* U, const float* W, int64_t C,
     KS_CUDA(cudaGetLastError());
     int rc = launch_temporal(X, W, C, L, P, nt, lay.Q, lay.Lpad, Yt, nullptr, nullptr, stream);
     if (rc) return rc;
-    return sgemm_tn(Uq, Yt, B, K, L, lay.Q, ldb, stream);
+    return sgemm_tn(Uq, Yt, B, K, L, lay.Q, ldb, stream, tiled);
   }
   __nv_bfloat16* Uhl = cv.take<__nv_bfloat16>((size_t)lay.Kpad * lay.Q * 2);
   __nv_bfloat16* Yhl = cv.take<__nv_bfloat16>((size_t)lay.Lpad * lay.Q * 2);
@@ -352,7 +359,7 @@ int launch_project(const float* X, const float* U, const float* W, int64_t C,
   KS_CUDA(cudaGetLastError());
   int rc = launch_temporal(X, W, C, L, P, nt, lay.Q, lay.Lpad, nullptr, Yhi, Ylo, stream);
   if (rc) return rc;
-  return gemm_bf16x3(Uhi, Ulo, Yhi, Ylo, B, K, L, lay.Q, lay.Kpad, lay.Lpad, ldb, stream);
+  return gemm_bf16x3(Uhi, Ulo, Yhi, Ylo, B, K, L, lay.Q, lay.Kpad, lay.Lpad, ldb, tiled, stream);
 }
 
 }  // namespace ks

@@ -87,6 +87,36 @@ class _Workspace:
 _ws = _Workspace()
 
 
+class _TransposedCtc:
+    """The most recent ctc in the peel's layout, ctcT[k][j][lag] = ctc[j][k][lag].
+
+    `extract` matches every batch with the same ctc tensor; transposing it once
+    instead of per batch saves a full pass over K*K*(2nt+1) floats per batch.
+    The entry is keyed by storage address, shape and the tensor's version
+    counter, so an in-place change of ctc invalidates it.
+    """
+
+    def __init__(self):
+        self._key = None
+        self._val = None
+
+    def get(self, ctc: torch.Tensor, nt: int) -> torch.Tensor:
+        key = (ctc.data_ptr(), tuple(ctc.shape), ctc.device, ctc._version)
+        if self._key == key:
+            return self._val
+        self._key, self._val = None, None
+        K = ctc.shape[0]
+        out = torch.empty_like(ctc)
+        lib = _lib.load()
+        _lib.check(lib.ks_ctc_transpose(_ptr(ctc), K, nt, _ptr(out), _stream(ctc.device)),
+                   "ks_ctc_transpose")
+        self._key, self._val = key, out
+        return out
+
+
+_ctcT = _TransposedCtc()
+
+
 def th2_of(Th) -> float:
     """Th_learned**2 as the reference's float32 comparison sees it."""
     return float(np.float32(float(Th) ** 2))
@@ -104,8 +134,12 @@ def template_energy(U: torch.Tensor) -> torch.Tensor:
     return nm
 
 
-def project_scores(X, U, W, nt, projection="fp32"):
-    """Score matrix B [K, L] (kilosort/template_matching.py:180-181)."""
+def project_scores(X, U, W, nt, projection="fp32", tiled=False):
+    """Score matrix B (kilosort/template_matching.py:180-181).
+
+    Returns B [K, L] (a view of a row-padded buffer), or with ``tiled`` the
+    peel's blocked layout Bt [ceil(L/32), K, 32], Bt[b, k, i] = B[k, 32*b + i].
+    """
     X = _need(X, "X", ndim=2)
     U = _need(U, "U", ndim=3)
     W = _need(W, "wPCA", ndim=2)
@@ -115,14 +149,19 @@ def project_scores(X, U, W, nt, projection="fp32"):
         raise ValueError("shape mismatch between X, U and wPCA")
     prec = _PROJECTIONS[projection]
     lib = _lib.load()
-    ldb = ((L + 63) // 64) * 64
-    B = torch.empty((K, ldb), dtype=torch.float32, device=X.device)
+    if tiled:
+        B = torch.empty(((L + 31) // 32, K, 32), dtype=torch.float32, device=X.device)
+        ldb, layout = 0, _lib.KS_B_TILED
+    else:
+        ldb = ((L + 63) // 64) * 64
+        B = torch.empty((K, ldb), dtype=torch.float32, device=X.device)
+        layout = _lib.KS_B_ROWS
     nbytes = lib.ks_project_workspace_size(Cn, L, K, P, prec)
     ws = _ws.get(X.device, nbytes)
     _lib.check(lib.ks_project(_ptr(X), _ptr(U), _ptr(W), Cn, L, K, P, nt, prec,
-                              _ptr(B), ldb, _ptr(ws), ws.numel(), _stream(X.device)),
+                              _ptr(B), ldb, layout, _ptr(ws), ws.numel(), _stream(X.device)),
                "ks_project")
-    return B[:, :L]
+    return B if tiled else B[:, :L]
 
 
 def _info_status(info, what):
@@ -137,16 +176,16 @@ def _info_status(info, what):
     return n, iters
 
 
-def peel(B, Xres, U, W, ctc, nm, Th, nt, max_peels, capacity=DEFAULT_CAPACITY):
+def peel(B, Xres, U, W, ctc, nm, Th, nt, max_peels, capacity=DEFAULT_CAPACITY,
+         ctc_transposed=False):
     """Greedy peel on a given score matrix, in place on B and Xres.
 
+    ``B`` is either [K, L] with contiguous rows (any row stride) or the tiled
+    [ceil(L/32), K, 32] layout of ``project_scores(..., tiled=True)``.  ``ctc``
+    is in the reference layout, or ctcT[k][j][lag] with ``ctc_transposed``.
     Returns (st [N,2] int64, amps [N,1], th_amps [N,1], iterations), in the
     order of kilosort/template_matching.py:183-244.
     """
-    if not (isinstance(B, torch.Tensor) and B.is_cuda and B.dtype == torch.float32
-            and B.dim() == 2 and B.stride(1) == 1 and B.stride(0) >= B.shape[1]):
-        raise ValueError("B must be a float32 CUDA matrix with contiguous rows")
-    ldb = B.stride(0)
     Xres = _need(Xres, "Xres", ndim=2)
     U = _need(U, "U", ndim=3)
     W = _need(W, "wPCA", ndim=2)
@@ -154,21 +193,43 @@ def peel(B, Xres, U, W, ctc, nm, Th, nt, max_peels, capacity=DEFAULT_CAPACITY):
     nm = _need(nm, "nm", ndim=1)
     K, P, Cn = U.shape
     L = Xres.shape[1]
-    if B.shape != (K, L) or ctc.shape != (K, K, 2 * nt + 1):
-        raise ValueError("shape mismatch between B, U, ctc and Xres")
+    if not (isinstance(B, torch.Tensor) and B.is_cuda and B.dtype == torch.float32):
+        raise ValueError("B must be a float32 CUDA tensor")
+    if B.dim() == 3:
+        if B.shape != ((L + 31) // 32, K, 32) or not B.is_contiguous():
+            raise ValueError("tiled B must be a contiguous [ceil(L/32), K, 32] tensor")
+        ldb, layout = 0, _lib.KS_B_TILED
+    else:
+        if not (B.dim() == 2 and B.shape == (K, L) and B.stride(1) == 1
+                and B.stride(0) >= L):
+            raise ValueError("B must be [K, L] with contiguous rows")
+        ldb, layout = B.stride(0), _lib.KS_B_ROWS
+    if ctc.shape != (K, K, 2 * nt + 1):
+        raise ValueError("shape mismatch between U and ctc")
+    clayout = _lib.KS_CTC_KJL if ctc_transposed else _lib.KS_CTC_JKL
     dev = Xres.device
     st = torch.zeros((capacity, 2), dtype=torch.int64, device=dev)
     amps = torch.zeros((capacity, 1), dtype=torch.float32, device=dev)
     th_amps = torch.zeros((capacity, 1), dtype=torch.float32, device=dev)
     info = torch.zeros(4, dtype=torch.int64, device=dev)
     lib = _lib.load()
-    ws = _ws.get(dev, lib.ks_peel_workspace_size(L, K))
-    _lib.check(lib.ks_peel(_ptr(B), ldb, _ptr(Xres), _ptr(U), _ptr(W), _ptr(ctc), _ptr(nm),
-                           Cn, L, K, P, nt, th2_of(Th), int(max_peels), int(capacity),
-                           _ptr(st), _ptr(amps), _ptr(th_amps), _ptr(info),
+    ws = _ws.get(dev, lib.ks_peel_workspace_size(L, K, nt, layout, clayout))
+    _lib.check(lib.ks_peel(_ptr(B), ldb, layout, _ptr(Xres), _ptr(U), _ptr(W), _ptr(ctc),
+                           clayout, _ptr(nm), Cn, L, K, P, nt, th2_of(Th), int(max_peels),
+                           int(capacity), _ptr(st), _ptr(amps), _ptr(th_amps), _ptr(info),
                            _ptr(ws), ws.numel(), _stream(dev)), "ks_peel")
     n, iters = _info_status(info, "ks_peel")
     return st[:n], amps[:n], th_amps[:n], iters
+
+
+def transpose_ctc(ctc, nt):
+    """ctcT[k][j][lag] = ctc[j][k][lag], the layout the peel streams."""
+    ctc = _need(ctc, "ctc", ndim=3)
+    out = torch.empty_like(ctc)
+    lib = _lib.load()
+    _lib.check(lib.ks_ctc_transpose(_ptr(ctc), ctc.shape[0], nt, _ptr(out),
+                                    _stream(ctc.device)), "ks_ctc_transpose")
+    return out
 
 
 # ------------------------------------------------------------------ drop-in API
@@ -204,8 +265,11 @@ def run_matching(ops, X, U, ctc, device=torch.device("cuda")):
     Xres = torch.empty_like(X)
     info = torch.zeros(4, dtype=torch.int64, device=dev)
     lib = _lib.load()
-    ws = _ws.get(dev, lib.ks_run_matching_workspace_size(Cn, L, K, P, prec))
-    _lib.check(lib.ks_run_matching(_ptr(X), _ptr(U), _ptr(W), _ptr(ctc), Cn, L, K, P, nt,
+    ctcT = _ctcT.get(ctc, nt)
+    ws = _ws.get(dev, lib.ks_run_matching_workspace_size(Cn, L, K, P, nt, prec,
+                                                         _lib.KS_CTC_KJL))
+    _lib.check(lib.ks_run_matching(_ptr(X), _ptr(U), _ptr(W), _ptr(ctcT), _lib.KS_CTC_KJL,
+                                   Cn, L, K, P, nt,
                                    th2_of(Th), max_peels, prec, capacity, _ptr(st),
                                    _ptr(amps), _ptr(th_amps), _ptr(Xres), _ptr(info),
                                    _ptr(ws), ws.numel(), _stream(dev)), "ks_run_matching")

@@ -33,8 +33,14 @@ def test_workspace_queries():
     # Yt: Lpad * Q floats (fp32) vs two bf16 planes -> same size; both > Y bytes
     assert fp32 >= 60160 * 2304 * 4
     assert split >= 60160 * 2304 * 4
-    assert lib.ks_peel_workspace_size(L, K) > 4 * L
-    total = lib.ks_run_matching_workspace_size(C, L, K, P, _lib.KS_PROJ_FP32)
+    peel = lib.ks_peel_workspace_size(L, K, 61, _lib.KS_B_ROWS, _lib.KS_CTC_KJL)
+    assert peel >= K * L * 4                     # tiled copy of a row-major B
+    assert lib.ks_peel_workspace_size(L, K, 61, _lib.KS_B_TILED, _lib.KS_CTC_KJL) < K * L
+    # the reference ctc layout adds room for its transposed copy
+    assert lib.ks_peel_workspace_size(L, K, 61, _lib.KS_B_ROWS, _lib.KS_CTC_JKL) >= \
+        peel + K * K * 123 * 4
+    total = lib.ks_run_matching_workspace_size(C, L, K, P, 61, _lib.KS_PROJ_FP32,
+                                               _lib.KS_CTC_KJL)
     assert total >= fp32 + K * L * 4
     assert lib.ks_ctc_workspace_size(K, P, C, 61) >= (K * P) ** 2 * 4
 
@@ -42,8 +48,8 @@ def test_workspace_queries():
 def test_peel_rejects_bad_arguments_before_touching_the_device():
     lib = _lib.load()
     # null pointers -> KS_ERR_ARG
-    rc = lib.ks_peel(None, 64, None, None, None, None, None, 4, 64, 2, 6, 61, 64.0,
-                     100, 10, None, None, None, None, None, 0, None)
+    rc = lib.ks_peel(None, 64, _lib.KS_B_ROWS, None, None, None, None, _lib.KS_CTC_JKL, None,
+                     4, 64, 2, 6, 61, 64.0, 100, 10, None, None, None, None, None, 0, None)
     assert rc == _lib.KS_ERR_ARG
     assert b"null" in lib.ks_last_error()
 

@@ -229,3 +229,18 @@ def test_cfg2_batch_fp32_vs_oracle(cuda_device):
     a = agreement(st.cpu().numpy(), st_r.numpy(), amps.cpu().numpy(), amps_r.numpy())
     assert a["agreement"] >= 0.995, a
     assert a["amp_rel_max"] <= 1e-4, a
+
+
+def test_tiled_scores_and_transposed_ctc(cuda_device):
+    """The peel's layouts hold the same numbers as the reference layouts."""
+    g = gu.load("small")
+    rec, X, U, W = gu.case_inputs(g)
+    Xd, Ud, Wd = (torch.from_numpy(a).to(DEV) for a in (X, U, W))
+    B = kb.project_scores(Xd, Ud, Wd, 61, "fp32")
+    Bt = kb.project_scores(Xd, Ud, Wd, 61, "fp32", tiled=True)
+    L = X.shape[1]
+    rebuilt = Bt.permute(1, 0, 2).reshape(U.shape[0], -1)[:, :L]
+    assert torch.equal(rebuilt, B)
+    ctc = torch.from_numpy(g["ctc_full"]).to(DEV)
+    ctcT = kb.transpose_ctc(ctc, 61)
+    assert torch.equal(ctcT, ctc.transpose(0, 1))
