@@ -70,13 +70,16 @@ KS_API int ks_template_energy(const float* U, int64_t K, int64_t P, int64_t C,
 /*
  * Score matrix B[k, tau] = sum_{p,c} U[k,p,c] * sum_t W[p,t] X[c, tau - nt/2 + t]
  * (zero padding), written in b_layout (row-major with ldb >= L, or tiled).
+ * status (device int, may be NULL) receives KS_OK or the device-side error of
+ * the contraction (KS_ERR_TIMEOUT if a bounded wait ran out; B is then
+ * undefined).
  * Replaces kilosort/template_matching.py:180-181 (conv1d + einsum).
  */
 KS_API size_t ks_project_workspace_size(int64_t C, int64_t L, int64_t K, int64_t P,
                                  int precision);
 KS_API int ks_project(const float* X, const float* U, const float* W,
                int64_t C, int64_t L, int64_t K, int64_t P, int64_t nt,
-               int precision, float* B, int64_t ldb, int b_layout,
+               int precision, float* B, int64_t ldb, int b_layout, int* status,
                void* workspace, size_t workspace_bytes, void* stream);
 
 /*

@@ -43,7 +43,7 @@ SIGNATURES = {
     "ks_template_energy": (_int, [_vp, _i64, _i64, _i64, _vp, _vp]),
     "ks_project_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _int]),
     "ks_project": (_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _int, _vp,
-                          _i64, _int, _vp, _sz, _vp]),
+                          _i64, _int, _vp, _vp, _sz, _vp]),
     "ks_peel_workspace_size": (_sz, [_i64, _i64, _i64, _int, _int]),
     "ks_peel": (_int, [_vp, _i64, _int, _vp, _vp, _vp, _vp, _int, _vp, _i64, _i64, _i64, _i64,
                        _i64, _f32, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),

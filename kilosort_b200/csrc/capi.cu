@@ -160,7 +160,7 @@ size_t ks_project_workspace_size(int64_t C, int64_t L, int64_t K, int64_t P,
 
 int ks_project(const float* X, const float* U, const float* W, int64_t C,
                int64_t L, int64_t K, int64_t P, int64_t nt, int precision,
-               float* B, int64_t ldb, int b_layout, void* workspace,
+               float* B, int64_t ldb, int b_layout, int* status, void* workspace,
                size_t workspace_bytes, void* stream) {
   if (!X || !U || !W || !B) return fail(KS_ERR_ARG, "ks_project: null pointer");
   if (b_layout != KS_B_ROWS && b_layout != KS_B_TILED)
@@ -169,7 +169,7 @@ int ks_project(const float* X, const float* U, const float* W, int64_t C,
   int rc = device_info(&d);
   if (rc) return rc;
   return launch_project(X, U, W, C, L, K, P, nt, precision, B, ldb, b_layout == KS_B_TILED,
-                        workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+                        workspace, workspace_bytes, status, static_cast<cudaStream_t>(stream));
 }
 
 size_t ks_peel_workspace_size(int64_t L, int64_t K, int64_t nt, int b_layout,
@@ -209,7 +209,7 @@ int ks_peel(float* B, int64_t ldb, int b_layout, float* Xres, const float* U, co
   }
   rc = launch_peel_tiled(Bt, Xres, U, W, ctcT, nm, C, L, K, P, nt, th2, max_peels, capacity,
                          st, amps, th_amps, info, base + m.peel_off, m.bytes - m.peel_off, s,
-                         wait_limit_ns());
+                         wait_limit_ns(), nullptr);
   if (rc) return rc;
   return b_layout == KS_B_ROWS ? launch_untile_rows(Bt, K, L, B, ldb, s) : KS_OK;
 }
@@ -252,11 +252,13 @@ int ks_run_matching(const float* X, const float* U, const float* W, const float*
   rc = launch_template_energy(U, K, P, C, nm, s);
   if (rc) return rc;
   rc = launch_project(X, U, W, C, L, K, P, nt, precision, Bt, 0, true, base + m.proj_off,
-                      m.ctc_off - m.proj_off, s);
+                      m.ctc_off - m.proj_off, nullptr, s);
   if (rc) return rc;
+  // the projection's error word is the first int of its workspace
   return launch_peel_tiled(Bt, Xres, U, W, ctcT, nm, C, L, K, P, nt, th2, max_peels,
                            capacity, st, amps, th_amps, info, base + m.peel_off,
-                           m.bytes - m.peel_off, s, wait_limit_ns());
+                           m.bytes - m.peel_off, s, wait_limit_ns(),
+                           reinterpret_cast<const int*>(base + m.proj_off));
 }
 
 int ks_ctc_transpose(const float* ctc, int64_t K, int64_t nt, float* ctcT, void* stream) {

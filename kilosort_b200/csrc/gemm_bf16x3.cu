@@ -1,11 +1,405 @@
-// Split-BF16 contraction on tcgen05 (placeholder until the tensor-core kernel lands).
+// Split-BF16 score contraction on the 5th-generation tensor cores (tcgen05).
+//
+//   B[k, tau] = sum_q U[k, q] * Y[tau, q]
+//             ~ Uhi.Yhi + Uhi.Ylo + Ulo.Yhi        (FP32 accumulate in TMEM)
+// with x = hi + lo, hi = bf16(x), lo = bf16(x - hi): the dropped lo.lo term and
+// the two roundings leave a relative error of about 2^-16 per product.
+//
+// Persistent kernel, one CTA per SM, 6 warps:
+//   warp 0     TMA producer: per 64-wide slice of q, four tiles (Uhi, Ulo
+//              128x64, Yhi, Ylo 256x64, bf16, 128-byte swizzle) into a 2-stage
+//              shared-memory ring (96 KB per stage), completion on an mbarrier
+//   warp 1     allocates 512 TMEM columns; one lane issues per slice 12 MMAs
+//              (3 products x 4 steps of K=16, M=128, N=256) into a double-
+//              buffered 128x256 FP32 accumulator and commits stage releases and
+//              accumulator hand-offs to mbarriers
+//   warps 2-5  epilogue: tcgen05.ld 32 columns at a time (one template row per
+//              thread) and store 128-byte rows of the output (row-major B, or
+//              the 32-column tiled layout of the peel, where a warp's 32 rows
+//              are one contiguous 4 KB run)
+// Tiles are (128 templates) x (256 samples), template tiles of one sample tile
+// consecutive so concurrent CTAs share the Y tile through L2.  No TMA multicast.
+// Every mbarrier wait is bounded by %globaltimer; a wait that runs out sets the
+// error word, the CTA drains its own copies in flight (bounded), frees TMEM and
+// returns.
 #include "ks_common.cuh"
 #include "project.cuh"
 
-namespace ks {
-int gemm_bf16x3(const __nv_bfloat16*, const __nv_bfloat16*, const __nv_bfloat16*,
-                const __nv_bfloat16*, float*, int64_t, int64_t, int64_t, int64_t,
-                int64_t, int64_t, bool, cudaStream_t) {
-  return fail(KS_ERR_UNSUPPORTED, "split-BF16 projection not built yet");
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+namespace {
+
+constexpr int kBM = 128;              // templates per tile (TMEM lanes)
+constexpr int kBN = 256;              // samples per tile (TMEM columns)
+constexpr int kBK = 64;               // q per slice: one 128-byte swizzle row
+constexpr int kStages = 2;
+constexpr int kTileA = kBM * kBK * 2;             // 16 KB
+constexpr int kTileB = kBN * kBK * 2;             // 32 KB
+constexpr int kStageBytes = 2 * kTileA + 2 * kTileB;
+constexpr int kThreads = 192;
+constexpr int kTmemCols = 512;
+constexpr unsigned long long kLimitNs = 2000000000ull;
+
+// instruction descriptor: FP32 accumulate, BF16 A and B, both K-major,
+// N = 256 (bits 17-22 hold N >> 3), M = 128 (bits 24-28 hold M >> 4)
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) |
+                            ((uint32_t)(kBM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase of the given parity; false (and the error word
+// set) when it runs out.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = ks_globaltimer();
+  while (!mbar_try_wait(bar, parity)) {
+    if (ks_ld_volatile(err) != 0) return false;
+    if (ks_globaltimer() - t0 > kLimitNs) {
+      atomicCAS(err, 0, KS_ERR_TIMEOUT);
+      return false;
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), version 1
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3fff);
+  d |= (uint64_t)1 << 16;                    // LBO (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;          // SBO
+  d |= (uint64_t)1 << 46;                    // version
+  d |= (uint64_t)2 << 61;                    // SWIZZLE_128B
+  return d;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   bar)
+               : "memory");
+}
+__device__ __forceinline__ void fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct GemmArgs {
+  float* B;
+  long long ldb;
+  int tiled;
+  int K, L, nk, tiles_m, n_tiles;
+  int* err;
+};
+
+__global__ void __launch_bounds__(kThreads, 1)
+ks_bf16x3_kernel(const __grid_constant__ CUtensorMap map_uhi,
+                 const __grid_constant__ CUtensorMap map_ulo,
+                 const __grid_constant__ CUtensorMap map_yhi,
+                 const __grid_constant__ CUtensorMap map_ylo, GemmArgs g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // 1024-byte alignment for the swizzled tiles
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  unsigned char* gbase = smem_raw + (base - raw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kStages * kStageBytes);
+  // bars: full[kStages], empty[kStages], tfull[2], tempty[2], drain[1]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 5);
+  const uint32_t full0 = smem_u32(bars);
+  const uint32_t empty0 = full0 + 8 * kStages;
+  const uint32_t tfull0 = empty0 + 8 * kStages;
+  const uint32_t tempty0 = tfull0 + 16;
+  const uint32_t drain = tempty0 + 16;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(tfull0 + 8 * a, 1);
+      mbar_init(tempty0 + 8 * a, 4);
+    }
+    mbar_init(drain, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
+
+  if (warp == 0) {
+    // ---------------------------------------------------------- TMA producer
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool pending[kStages] = {};     // a load was issued into the stage ...
+      uint32_t pend_ph[kStages] = {}; // ... completing this phase of full[stage]
+      bool ok = true;
+      for (int t = blockIdx.x; ok && t < g.n_tiles; t += gridDim.x) {
+        const int m0 = (t % g.tiles_m) * kBM;
+        const int n0 = (t / g.tiles_m) * kBN;
+        for (int kb = 0; kb < g.nk; ++kb) {
+          if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, g.err)) { ok = false; break; }
+          const uint32_t st = base + s * kStageBytes;
+          const uint32_t fb = full0 + 8 * s;
+          mbar_expect_tx(fb, kStageBytes);
+          tma_load_2d(st, &map_uhi, kb * kBK, m0, fb);
+          tma_load_2d(st + kTileA, &map_ulo, kb * kBK, m0, fb);
+          tma_load_2d(st + 2 * kTileA, &map_yhi, kb * kBK, n0, fb);
+          tma_load_2d(st + 2 * kTileA + kTileB, &map_ylo, kb * kBK, n0, fb);
+          pending[s] = true;
+          pend_ph[s] = ph;
+          if (++s == kStages) { s = 0; ph ^= 1u; }
+        }
+      }
+      if (!ok) {
+        // leave no copy in flight: wait (bounded) for the last load of each stage
+        const unsigned long long t0 = ks_globaltimer();
+        for (int si = 0; si < kStages; ++si) {
+          if (!pending[si]) continue;
+          while (!mbar_try_wait(full0 + 8 * si, pend_ph[si])) {
+            if (ks_globaltimer() - t0 > kLimitNs) break;
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      int acc = 0;
+      uint32_t acc_ph = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; ok && t < g.n_tiles; t += gridDim.x) {
+        if (!mbar_wait(tempty0 + 8 * acc, acc_ph ^ 1u, g.err)) { ok = false; break; }
+        fence_after();
+        const uint32_t d = tmem + (uint32_t)(acc * kBN);
+        for (int kb = 0; kb < g.nk; ++kb) {
+          if (!mbar_wait(full0 + 8 * s, ph, g.err)) { ok = false; break; }
+          fence_after();
+          const uint32_t st = base + s * kStageBytes;
+#pragma unroll
+          for (int kk = 0; kk < kBK / 16; ++kk) {
+            const uint64_t a_hi = smem_desc(st + kk * 32);
+            const uint64_t a_lo = smem_desc(st + kTileA + kk * 32);
+            const uint64_t b_hi = smem_desc(st + 2 * kTileA + kk * 32);
+            const uint64_t b_lo = smem_desc(st + 2 * kTileA + kTileB + kk * 32);
+            const uint32_t first = (kb == 0 && kk == 0) ? 0u : 1u;
+            mma_bf16(d, a_hi, b_hi, first);
+            mma_bf16(d, a_hi, b_lo, 1u);
+            mma_bf16(d, a_lo, b_hi, 1u);
+          }
+          mma_commit(empty0 + 8 * s);   // stage free once these MMAs finish
+          if (++s == kStages) { s = 0; ph ^= 1u; }
+        }
+        if (!ok) break;
+        mma_commit(tfull0 + 8 * acc);   // accumulator complete
+        acc ^= 1;
+        if (acc == 0) acc_ph ^= 1u;
+      }
+      // every MMA issued by this thread has completed once this commit lands
+      mma_commit(drain);
+      const unsigned long long t0 = ks_globaltimer();
+      while (!mbar_try_wait(drain, 0u)) {
+        if (ks_globaltimer() - t0 > kLimitNs) break;
+      }
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue
+    const int q = warp & 3;                  // TMEM lane quadrant of this warp
+    int acc = 0;
+    uint32_t acc_ph = 0;
+    for (int t = blockIdx.x; t < g.n_tiles; t += gridDim.x) {
+      const int m0 = (t % g.tiles_m) * kBM;
+      const int n0 = (t / g.tiles_m) * kBN;
+      if (!mbar_wait(tfull0 + 8 * acc, acc_ph, g.err)) break;
+      fence_after();
+      const int row = m0 + q * 32 + lane;    // template of this thread
+      const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kBN);
+#pragma unroll 1
+      for (int c = 0; c < kBN / 32; ++c) {
+        uint32_t r[32];
+        tmem_ld32(tl + (uint32_t)(c * 32), r);
+        const int n = n0 + c * 32;
+        if (row < g.K && n < g.L) {
+          float* dst = g.tiled ? g.B + ((size_t)(n >> 5) * g.K + row) * 32
+                               : g.B + (size_t)row * g.ldb + n;
+          const bool full = n + 32 <= g.L && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
+          if (full) {
+#pragma unroll
+            for (int v = 0; v < 8; ++v)
+              reinterpret_cast<float4*>(dst)[v] =
+                  make_float4(__uint_as_float(r[4 * v]), __uint_as_float(r[4 * v + 1]),
+                              __uint_as_float(r[4 * v + 2]), __uint_as_float(r[4 * v + 3]));
+          } else {
+#pragma unroll
+            for (int e = 0; e < 32; ++e)
+              if (n + e < g.L) dst[e] = __uint_as_float(r[e]);
+          }
+        }
+      }
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tempty0 + 8 * acc);
+      acc ^= 1;
+      if (acc == 0) acc_ph ^= 1u;
+    }
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTmemCols)
+                 : "memory");
+  }
+}
+
+// ------------------------------------------------------------------ host side
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<EncodeTiled>(nullptr);
+    return reinterpret_cast<EncodeTiled>(p);
+  }();
+  return fn;
+}
+
+// 2-D bf16 tensor [rows][cols] (cols contiguous), box [box_rows][64], 128B swizzle
+int make_map(CUtensorMap* map, const __nv_bfloat16* ptr, int64_t rows, int64_t cols,
+             int box_rows) {
+  EncodeTiled fn = encode_fn();
+  if (!fn) return ks::fail(KS_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return ks::fail(KS_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  return KS_OK;
+}
+
+}  // namespace
+
+namespace ks {
+
+int gemm_bf16x3(const __nv_bfloat16* Uhi, const __nv_bfloat16* Ulo, const __nv_bfloat16* Yhi,
+                const __nv_bfloat16* Ylo, float* B, int64_t K, int64_t L, int64_t Q,
+                int64_t Kpad, int64_t Lpad, int64_t ldb, bool tiled, int* err,
+                cudaStream_t stream) {
+  if (!err) return fail(KS_ERR_ARG, "bf16x3: error word missing");
+  if (Q % kBK) return fail(KS_ERR_ARG, "bf16x3: contraction length must be a multiple of 64");
+  if (Kpad % kBM) return fail(KS_ERR_ARG, "bf16x3: template rows must be padded to 128");
+  const uintptr_t al = reinterpret_cast<uintptr_t>(Uhi) | reinterpret_cast<uintptr_t>(Ulo) |
+                       reinterpret_cast<uintptr_t>(Yhi) | reinterpret_cast<uintptr_t>(Ylo);
+  if (al & 15) return fail(KS_ERR_ARG, "bf16x3: operands must be 16-byte aligned");
+  DeviceInfo dev;
+  int rc = device_info(&dev);
+  if (rc) return rc;
+  CUtensorMap m_uhi, m_ulo, m_yhi, m_ylo;
+  if ((rc = make_map(&m_uhi, Uhi, Kpad, Q, kBM))) return rc;
+  if ((rc = make_map(&m_ulo, Ulo, Kpad, Q, kBM))) return rc;
+  if ((rc = make_map(&m_yhi, Yhi, Lpad, Q, kBN))) return rc;
+  if ((rc = make_map(&m_ylo, Ylo, Lpad, Q, kBN))) return rc;
+  GemmArgs g;
+  g.B = B;
+  g.ldb = ldb;
+  g.tiled = tiled ? 1 : 0;
+  g.K = (int)K;
+  g.L = (int)L;
+  g.nk = (int)(Q / kBK);
+  g.tiles_m = (int)(Kpad / kBM);
+  g.n_tiles = g.tiles_m * (int)((L + kBN - 1) / kBN);
+  g.err = err;
+  const size_t smem = (size_t)kStages * kStageBytes + 1024 + 256;
+  static int attr_device = -1;
+  if (attr_device != dev.device) {
+    KS_CUDA(cudaFuncSetAttribute(ks_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    attr_device = dev.device;
+  }
+  const int grid = std::min(dev.sm_count, g.n_tiles);
+  ks_bf16x3_kernel<<<grid, kThreads, smem, stream>>>(m_uhi, m_ulo, m_yhi, m_ylo, g);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
 }  // namespace ks

@@ -108,6 +108,7 @@ struct PeelArgs {
   unsigned* wctr;             // [2] work counters
   unsigned* bar;              // {count, generation}
   int* err;
+  const int* upstream_err;    // error word of the producer of Bt (may be null)
   int nchunks, nblk, nwords;
   unsigned long long limit_ns;
 };
@@ -524,6 +525,11 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
   const long long gwarp = (long long)blockIdx.x * kWarps + warp;
   const long long nwarps = (long long)G * kWarps;
   for (int i = tid; i < a.P * a.nt; i += kThreads) s.W[i] = a.W[i];
+  // a failed producer of the score matrix fails the peel
+  if (blockIdx.x == 0 && tid == 0 && a.upstream_err) {
+    const int ue = ks_ld_volatile(a.upstream_err);
+    if (ue) atomicCAS(a.err, 0, ue);
+  }
   __syncthreads();
 
   // initial scores of every column, folded into pack[1] (zeroed by the host)
@@ -733,7 +739,7 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
                       int64_t P, int64_t nt, float th2, int64_t max_peels,
                       int64_t capacity, int64_t* st, float* amps, float* th_amps,
                       int64_t* info, void* ws, size_t ws_bytes, cudaStream_t stream,
-                      unsigned long long limit_ns) {
+                      unsigned long long limit_ns, const int* upstream_err) {
   if (!Bt || !Xres || !U || !W || !ctcT || !nm || !st || !amps || !th_amps || !info)
     return fail(KS_ERR_ARG, "ks_peel: null pointer");
   if (C < 1 || L < 1 || K < 1 || P < 1 || nt < 1 || (nt % 2) == 0)
@@ -776,6 +782,7 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
   a.touch = cv.take<Touch>(2 * (size_t)lay.nblk * kTouch);
   a.nchunks = lay.nchunks; a.nblk = lay.nblk; a.nwords = lay.nwords;
   a.limit_ns = limit_ns;
+  a.upstream_err = upstream_err;
 
   const size_t smem = smem_bytes(a.P, a.nt, a.nchunks, a.nwords);
   if (smem > dev.smem_optin) return fail(KS_ERR_UNSUPPORTED, "ks_peel: batch too long for shared memory");

@@ -262,6 +262,7 @@ ProjLayout proj_layout(int64_t C, int64_t L, int64_t K, int64_t P, int precision
   l.Lpad = round_up(L, 128);
   l.Kpad = round_up(K, 128);
   Carve cv(nullptr);
+  cv.take<int>(64);   // error word
   if (precision == KS_PROJ_FP32) {
     cv.take<float>((size_t)l.Kpad * l.Q);
     cv.take<float>((size_t)l.Lpad * l.Q);
@@ -325,7 +326,7 @@ int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
 int launch_project(const float* X, const float* U, const float* W, int64_t C,
                    int64_t L, int64_t K, int64_t P, int64_t nt, int precision,
                    float* B, int64_t ldb, bool tiled, void* ws, size_t ws_bytes,
-                   cudaStream_t stream) {
+                   int* err_out, cudaStream_t stream) {
   if (!X || !U || !W || !B) return fail(KS_ERR_ARG, "ks_project: null pointer");
   if (C < 1 || L < 1 || K < 1 || P < 1 || nt < 1 || (nt % 2) == 0)
     return fail(KS_ERR_ARG, "ks_project: need C,L,K,P >= 1 and odd nt");
@@ -337,6 +338,8 @@ int launch_project(const float* X, const float* U, const float* W, int64_t C,
   const ProjLayout lay = proj_layout(C, L, K, P, precision);
   if (!ws || ws_bytes < lay.bytes) return fail(KS_ERR_WORKSPACE, "ks_project: workspace too small");
   Carve cv(ws);
+  int* err = cv.take<int>(64);
+  KS_CUDA(cudaMemsetAsync(err, 0, sizeof(int), stream));
   const int reorder_blocks = (int)std::min<int64_t>(4096, (lay.Kpad * lay.Q + 255) / 256);
   if (precision == KS_PROJ_FP32) {
     float* Uq = cv.take<float>((size_t)lay.Kpad * lay.Q);
@@ -346,7 +349,10 @@ int launch_project(const float* X, const float* U, const float* W, int64_t C,
     KS_CUDA(cudaGetLastError());
     int rc = launch_temporal(X, W, C, L, P, nt, lay.Q, lay.Lpad, Yt, nullptr, nullptr, stream);
     if (rc) return rc;
-    return sgemm_tn(Uq, Yt, B, K, L, lay.Q, ldb, stream, tiled);
+    rc = sgemm_tn(Uq, Yt, B, K, L, lay.Q, ldb, stream, tiled);
+    if (rc) return rc;
+    if (err_out) KS_CUDA(cudaMemcpyAsync(err_out, err, sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    return KS_OK;
   }
   __nv_bfloat16* Uhl = cv.take<__nv_bfloat16>((size_t)lay.Kpad * lay.Q * 2);
   __nv_bfloat16* Yhl = cv.take<__nv_bfloat16>((size_t)lay.Lpad * lay.Q * 2);
@@ -359,7 +365,10 @@ int launch_project(const float* X, const float* U, const float* W, int64_t C,
   KS_CUDA(cudaGetLastError());
   int rc = launch_temporal(X, W, C, L, P, nt, lay.Q, lay.Lpad, nullptr, Yhi, Ylo, stream);
   if (rc) return rc;
-  return gemm_bf16x3(Uhi, Ulo, Yhi, Ylo, B, K, L, lay.Q, lay.Kpad, lay.Lpad, ldb, tiled, stream);
+  rc = gemm_bf16x3(Uhi, Ulo, Yhi, Ylo, B, K, L, lay.Q, lay.Kpad, lay.Lpad, ldb, tiled, err, stream);
+  if (rc) return rc;
+  if (err_out) KS_CUDA(cudaMemcpyAsync(err_out, err, sizeof(int), cudaMemcpyDeviceToDevice, stream));
+  return KS_OK;
 }
 
 }  // namespace ks

@@ -18,17 +18,20 @@ int launch_template_energy(const float* U, int64_t K, int64_t P, int64_t C,
                            float* nm, cudaStream_t stream);
 // B is written row-major [K, ldb] or, when tiled, in 32-column blocks
 // [ceil(L/32)][K][32] (the layout of the peel).
+// The first 256 bytes of the workspace hold the device error word of the
+// tensor-core contraction (zeroed here); with err_out the word is also copied
+// there after the contraction.
 int launch_project(const float* X, const float* U, const float* W, int64_t C,
                    int64_t L, int64_t K, int64_t P, int64_t nt, int precision,
                    float* B, int64_t ldb, bool tiled, void* ws, size_t ws_bytes,
-                   cudaStream_t stream);
+                   int* err_out, cudaStream_t stream);
 int sgemm_tn(const float* A, const float* Bt, float* Cm, int64_t M, int64_t N,
              int64_t Kd, int64_t ldc, cudaStream_t stream, bool tiled);
 // Split-BF16 contraction on tcgen05: B = Uhi*Yhi^T + Uhi*Ylo^T + Ulo*Yhi^T.
 int gemm_bf16x3(const __nv_bfloat16* Uhi, const __nv_bfloat16* Ulo,
                 const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, float* B,
                 int64_t K, int64_t L, int64_t Q, int64_t Kpad, int64_t Lpad,
-                int64_t ldb, bool tiled, cudaStream_t stream);
+                int64_t ldb, bool tiled, int* err, cudaStream_t stream);
 
 // Peel on a tiled score matrix Bt [ceil(L/32)][K][32] and a transposed
 // cross-correlation ctcT[k][j][lag] = ctc[j][k][lag].
@@ -45,6 +48,6 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
                       int64_t P, int64_t nt, float th2, int64_t max_peels,
                       int64_t capacity, int64_t* st, float* amps, float* th_amps,
                       int64_t* info, void* ws, size_t ws_bytes, cudaStream_t stream,
-                      unsigned long long limit_ns);
+                      unsigned long long limit_ns, const int* upstream_err);
 
 }  // namespace ks

@@ -134,11 +134,12 @@ def template_energy(U: torch.Tensor) -> torch.Tensor:
     return nm
 
 
-def project_scores(X, U, W, nt, projection="fp32", tiled=False):
+def project_scores(X, U, W, nt, projection="fp32", tiled=False, check_status=True):
     """Score matrix B (kilosort/template_matching.py:180-181).
 
     Returns B [K, L] (a view of a row-padded buffer), or with ``tiled`` the
     peel's blocked layout Bt [ceil(L/32), K, 32], Bt[b, k, i] = B[k, 32*b + i].
+    ``check_status`` reads the device status (one host synchronisation).
     """
     X = _need(X, "X", ndim=2)
     U = _need(U, "U", ndim=3)
@@ -158,9 +159,15 @@ def project_scores(X, U, W, nt, projection="fp32", tiled=False):
         layout = _lib.KS_B_ROWS
     nbytes = lib.ks_project_workspace_size(Cn, L, K, P, prec)
     ws = _ws.get(X.device, nbytes)
+    status = torch.zeros(1, dtype=torch.int32, device=X.device)
     _lib.check(lib.ks_project(_ptr(X), _ptr(U), _ptr(W), Cn, L, K, P, nt, prec,
-                              _ptr(B), ldb, layout, _ptr(ws), ws.numel(), _stream(X.device)),
-               "ks_project")
+                              _ptr(B), ldb, layout, _ptr(status), _ptr(ws), ws.numel(),
+                              _stream(X.device)), "ks_project")
+    if check_status:
+        st = int(status.item())
+        if st != _lib.KS_OK:
+            raise _lib.KilosortB200Error(st, f"ks_project: device status {st} "
+                                         f"({_lib.status_message(st)})")
     return B if tiled else B[:, :L]
 
 
