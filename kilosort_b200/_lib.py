@@ -58,6 +58,8 @@ SIGNATURES = {
     "ks_ctc_workspace_size": (_sz, [_i64, _i64, _i64, _i64]),
     "ks_ctc": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp, _sz, _vp]),
     "ks_selftest_wait": (_int, [_i64, _vp, _vp]),
+    "ks_peel_static": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
+                              _f32, _i64, _i64, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None
