@@ -32,14 +32,18 @@
 //   UPDATE  every block computes the exclusive prefix of the chunk counts (a
 //           peak's global index in the iteration) and of the dirty bitmap.
 //           Records are written in (iteration, tau) order.  Warps take work
-//           items from a counter: (dirty block in column order, row range):
+//           items round-robin: (dirty block in column order, row range):
 //           B[j,c] -= amp*ctc[j,k,c-tau+nt] for the peaks touching column c,
 //           even-indexed peaks first, then odd-indexed -- the order of the
 //           reference's two interleaved groups (:235-238) -- product and
 //           difference rounded separately; rescored rows fold into pack[p].
-//           Then (peak, 8 channels) items update the residual windows (:237).
 // The loop ends when no peak is found or after max_peels iterations, decided
-// identically by every block from the same counts.  Every device-wide wait is
+// identically by every block from the same counts.  The residual (:237) is not
+// read inside the loop, so its updates run once afterwards: per 32-column
+// block the spikes whose windows cover it are gathered from the time-sorted
+// records of each iteration and subtracted element by element in record order,
+// the order of the reference's iterations; every element of Xres is read and
+// written once instead of once per touching spike.  Every device-wide wait is
 // bounded; a wait that runs out records KS_ERR_TIMEOUT and all blocks leave.
 #include "ks_common.cuh"
 #include "project.cuh"
@@ -50,12 +54,14 @@ constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kChunk = 256;          // detection chunk, one column per thread
 constexpr int kCol = 32;             // update block, one column per lane
-constexpr int kRowsPerWarp = 8;      // template rows in flight per lane
+constexpr int kRowsPerWarp = 16;     // template rows in flight per lane
 constexpr int kItemRows = 64;        // template rows per update item (at most)
 constexpr int kTouch = 8;            // peaks touching one block (more: ties)
-constexpr int kXresChans = 8;        // channels per residual item
-constexpr int kGrab = 2;             // work items taken per counter increment
 constexpr int kMaxChunks = 16384;
+constexpr int kMaxIters = 4096;      // iterations whose record offsets are kept
+constexpr int kMaxTemplates = 65536; // templates of one batch
+constexpr int kXList = 64;           // residual list entries per warp and epoch
+constexpr int kXCap = 32;            // spikes recorded per block for the residual
 
 // Phase timeline for profiling builds (-DKS_PEEL_TRACE): block 0 writes
 // %globaltimer stamps to info[8 + 8*it + slot]; the caller sizes info.
@@ -85,6 +91,7 @@ struct PeelArgs {
   const float* W;
   const float* ctcT;
   const float* nm;
+  const float2* nmi;          // {nm[j], 1/nm[j]} (1/nm NaN when nm is not a positive normal)
   int C, L, K, P, nt;
   float th2;
   int max_peels;
@@ -106,6 +113,9 @@ struct PeelArgs {
   Touch* touch;               // [2][nblk * kTouch]
   unsigned* dbits;            // [2][nwords]
   unsigned* wctr;             // [2] work counters
+  int* itoff;                 // [kMaxIters] first record of each iteration
+  int* xcount;                // [nblk] spikes whose residual window meets the block
+  int* xlist;                 // [nblk * kXCap] their record indices (unordered)
   unsigned* bar;              // {count, generation}
   int* err;
   const int* upstream_err;    // error word of the producer of Bt (may be null)
@@ -125,7 +135,6 @@ struct Smem {
   int* tl_tau;     // kWarps*kTouch   ordered touch list of each warp's item
   int* tl_k;       // kWarps*kTouch
   float* tl_amp;   // kWarps*kTouch
-  float* xu;       // kWarps*64       U values of a residual item
 };
 
 __device__ __forceinline__ Smem carve_smem(const PeelArgs& a, char* base) {
@@ -148,7 +157,6 @@ __device__ __forceinline__ Smem carve_smem(const PeelArgs& a, char* base) {
   s.tl_tau = reinterpret_cast<int*>(take(sizeof(int) * kWarps * kTouch));
   s.tl_k = reinterpret_cast<int*>(take(sizeof(int) * kWarps * kTouch));
   s.tl_amp = reinterpret_cast<float*>(take(sizeof(float) * kWarps * kTouch));
-  s.xu = reinterpret_cast<float*>(take(sizeof(float) * kWarps * 64));
   return s;
 }
 
@@ -158,7 +166,7 @@ size_t smem_bytes(int P, int nt, int nchunks, int nwords) {
   return r(sizeof(float) * P * nt) + r(sizeof(int) * (nchunks + 1)) +
          r(sizeof(int) * (nwords + 1)) + 3 * r(sizeof(float) * wn) +
          r(sizeof(int) * kChunk) + r(sizeof(int) * (kWarps + 1)) +
-         3 * r(sizeof(int) * kWarps * kTouch) + r(sizeof(float) * kWarps * 64);
+         3 * r(sizeof(int) * kWarps * kTouch);
 }
 
 __device__ __forceinline__ unsigned long long pack_score(float cf, int j) {
@@ -170,6 +178,26 @@ __device__ __forceinline__ float pack_value(unsigned long long v) {
 __device__ __forceinline__ int pack_index(unsigned long long v) {
   return (int)(~(unsigned)(v & 0xffffffffull));
 }
+// Fold row j's score relu(b)^2/nm[j] into (best, arg) -- larger score wins,
+// the earlier (smaller) row on ties -- computing the IEEE quotient only where
+// it can matter: sq*(1/nm) is within a relative 2^-22 of sq/nm, so a row whose
+// quotient could reach best has sq*(1/nm) >= best*(1 - 2^-20).  Rows failing
+// that test cannot change (best, arg).  The quotient itself is the exactly
+// rounded division, as in the reference.
+__device__ __forceinline__ void fold_score(float b, float2 nmi, int j, float& best, int& arg) {
+  const float rl = b > 0.f ? b : 0.f;
+  const float sq = __fmul_rn(rl, rl);
+  const float approx = __fmul_rn(sq, nmi.y);
+  const bool maybe = best < 0.f || !(approx < best * 0.99999905f) || approx != approx;
+  if (maybe) {
+    const float cf = __fdiv_rn(sq, nmi.x);
+    if (cf > best) {
+      best = cf;
+      arg = j;
+    }
+  }
+}
+
 __device__ __forceinline__ const float* bt_row(const PeelArgs& a, int blk, int j) {
   return a.Bt + ((size_t)blk * a.K + j) * kCol;
 }
@@ -378,50 +406,48 @@ __device__ __forceinline__ TouchList load_touch_warp(const PeelArgs& a, const Sm
 }
 
 // Columns of block blk x template rows [j_lo, j_hi): subtract the touching
-// peaks, store the changed rows, fold the rescored rows into pack_out.  A
-// column is touched by at most two peaks unless scores tie exactly; those two
-// are loaded with the rows of B so a group of rows costs one round trip.
+// peaks, store the changed rows, fold the rescored rows into pack_out.  Most
+// columns are touched by one peak; its cross-correlations are loaded with the
+// rows of B (16 rows per round trip).  Later peaks of the same column (at
+// most one more unless scores tie exactly) are applied in a second round, in
+// the same order.
 __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk,
                                  int j_lo, int j_hi, unsigned long long* pack_out,
                                  int lane) {
   const int c = blk * kCol + lane;
   const bool colok = c < a.L;
   const int nt = a.nt, K = a.K, nlag = 2 * nt + 1;
-  int e0 = -1, e1 = -1;
+  int e0 = -1;
   unsigned rest = 0u;                                 // further touching entries
   for (int e = 0; e < tl.n; ++e) {
     const int d = c - tl.tau[e];
     if (colok && d >= -nt && d <= nt) {
       if (e0 < 0) e0 = e;
-      else if (e1 < 0) e1 = e;
       else rest |= 1u << e;
     }
   }
   const bool touched = e0 >= 0;
+  const bool any_rest = __any_sync(0xffffffffu, rest != 0u);
   const float* cp0 = a.ctcT;
-  const float* cp1 = a.ctcT;
-  float amp0 = 0.f, amp1 = 0.f;
+  float amp0 = 0.f;
   if (e0 >= 0) { cp0 = a.ctcT + (size_t)tl.k[e0] * K * nlag + (c - tl.tau[e0] + nt); amp0 = tl.amp[e0]; }
-  if (e1 >= 0) { cp1 = a.ctcT + (size_t)tl.k[e1] * K * nlag + (c - tl.tau[e1] + nt); amp1 = tl.amp[e1]; }
   float* bcol = a.Bt + (size_t)blk * K * kCol + lane;
   float best = -1.f;
   int arg = 0;
   for (int j0 = j_lo; j0 < j_hi; j0 += kRowsPerWarp) {
-    float bv[kRowsPerWarp], w0[kRowsPerWarp], w1[kRowsPerWarp];
+    float bv[kRowsPerWarp], w0[kRowsPerWarp];
 #pragma unroll
     for (int r = 0; r < kRowsPerWarp; ++r) {
       const int j = j0 + r;
       const bool ok = colok && j < j_hi;
       bv[r] = ok ? bcol[(size_t)j * kCol] : 0.f;
       w0[r] = (ok && e0 >= 0) ? __ldg(cp0 + (size_t)j * nlag) : 0.f;
-      w1[r] = (ok && e1 >= 0) ? __ldg(cp1 + (size_t)j * nlag) : 0.f;
     }
+    if (e0 >= 0) {
 #pragma unroll
-    for (int r = 0; r < kRowsPerWarp; ++r) {
-      if (e0 >= 0) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp0, w0[r]));
-      if (e1 >= 0) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp1, w1[r]));
+      for (int r = 0; r < kRowsPerWarp; ++r) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp0, w0[r]));
     }
-    if (rest) {
+    if (any_rest) {
       for (int e = 0; e < tl.n; ++e) {
         if ((rest >> e) & 1u) {
           const float amp = tl.amp[e];
@@ -429,8 +455,10 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
 #pragma unroll
           for (int r = 0; r < kRowsPerWarp; ++r) {
             const int j = j0 + r;
-            if (j < j_hi) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp, __ldg(cp + (size_t)j * nlag)));
+            w0[r] = (j < j_hi) ? __ldg(cp + (size_t)j * nlag) : 0.f;
           }
+#pragma unroll
+          for (int r = 0; r < kRowsPerWarp; ++r) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp, w0[r]));
         }
       }
     }
@@ -439,67 +467,11 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
       const int j = j0 + r;
       if (colok && j < j_hi) {
         if (touched) bcol[(size_t)j * kCol] = bv[r];
-        const float rl = bv[r] > 0.f ? bv[r] : 0.f;
-        const float cf = __fdiv_rn(__fmul_rn(rl, rl), __ldg(a.nm + j));
-        if (cf > best) {
-          best = cf;
-          arg = j;
-        }
+        fold_score(bv[r], __ldg(a.nmi + j), j, best, arg);
       }
     }
   }
   if (colok && best >= 0.f) atomicMax(&pack_out[c], pack_score(best, arg));
-}
-
-// Subtract amp * sum_p U[k,p,c] W[p,t] from Xres[c, tau - nt/2 + t] for 8
-// channels of one peak; lanes run along t.  The U values of the 8 channels go
-// through the warp's shared-memory slot and all residual values of a 64-tap
-// span are loaded before any is written.
-__device__ void xres_warp_item(const PeelArgs& a, const Smem& s, int sp, int cg,
-                               int lane, int warp) {
-  int lo = 0, hi = a.nchunks - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (s.prefix[mid] <= sp) lo = mid; else hi = mid - 1;
-  }
-  const long long slot = (long long)lo * kChunk + (sp - s.prefix[lo]);
-  const int tau = a.chunk_tau[slot];
-  const int k = a.chunk_k[slot];
-  const float amp = a.chunk_amp[slot];
-  const int nt = a.nt, P = a.P;
-  const int t0 = tau - nt / 2;
-  const int cbase = cg * kXresChans;
-  const int nch = min(kXresChans, a.C - cbase);
-  float* su = s.xu + warp * kXresChans * 8;       // [channel][component]
-  __syncwarp();
-  for (int e = lane; e < kXresChans * 8; e += 32) {
-    const int ci = e >> 3, pp = e & 7;
-    su[e] = (ci < nch && pp < P) ? __ldg(a.U + ((long long)k * P + pp) * a.C + cbase + ci) : 0.f;
-  }
-  __syncwarp();
-  for (int tb = 0; tb < nt; tb += 64) {
-    float xv[kXresChans][2];
-#pragma unroll
-    for (int ci = 0; ci < kXresChans; ++ci)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int t = tb + lane + 32 * h;
-        xv[ci][h] = (ci < nch && t < nt) ? a.Xres[(long long)(cbase + ci) * a.L + t0 + t] : 0.f;
-      }
-#pragma unroll
-    for (int ci = 0; ci < kXresChans; ++ci)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int t = tb + lane + 32 * h;
-        if (ci < nch && t < nt) {
-          float wv = 0.f;
-#pragma unroll
-          for (int pp = 0; pp < 8; ++pp)
-            if (pp < P) wv = fmaf(su[ci * 8 + pp], s.W[pp * nt + t], wv);
-          a.Xres[(long long)(cbase + ci) * a.L + t0 + t] = __fsub_rn(xv[ci][h], __fmul_rn(amp, wv));
-        }
-      }
-  }
 }
 
 // Block of the rank-th set bit of the dirty bitmap (s.wprefix holds the
@@ -573,10 +545,17 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
       for (int i = tid; i < c_n; i += kThreads) {
         const long long slot = (long long)ch * kChunk + i;
         const long long o = n_out + s.prefix[ch] + i;
-        a.st[2 * o] = a.chunk_tau[slot];
+        const int tau = a.chunk_tau[slot];
+        a.st[2 * o] = tau;
         a.st[2 * o + 1] = a.chunk_k[slot];
         a.amps[o] = a.chunk_amp[slot];
         a.th_amps[o] = a.chunk_th[slot];
+        // blocks whose columns this spike's residual window covers
+        const int xb0 = (tau - a.nt / 2) / kCol, xb1 = (tau + a.nt / 2) / kCol;
+        for (int b = xb0; b <= xb1; ++b) {
+          const int pos = atomicAdd(&a.xcount[b], 1);
+          if (pos < kXCap) a.xlist[(size_t)b * kXCap + pos] = (int)o;
+        }
       }
     }
     // registration lists, bitmap and work counter of the next iteration start empty
@@ -586,37 +565,27 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
       a.dbits[(size_t)q * a.nwords + w] = 0u;
     if (blockIdx.x == 0 && tid == 0) a.wctr[q] = 0u;
     // update items: (dirty block in column order, row range), sized so that
-    // there are about four per warp; then residual items
+    // there are about four per warp
     int rows = kItemRows;
     if (ndirty > 0) {
       const long long per_blk = (4 * nwarps + ndirty - 1) / ndirty;   // items wanted per block
-      const int r = (int)((a.K + per_blk - 1) / per_blk);
+      int r = (int)((a.K + per_blk - 1) / per_blk);
+      r = (r + kRowsPerWarp - 1) / kRowsPerWarp * kRowsPerWarp;   // whole row groups
       rows = max(kRowsPerWarp, min(kItemRows, r));
     }
     const int rgroups = (a.K + rows - 1) / rows;
     const long long n_upd = (long long)ndirty * rgroups;
-    const int xgroups = (a.C + kXresChans - 1) / kXresChans;
-    const long long n_items = n_upd + (long long)total * xgroups;
+    const long long n_items = n_upd;
+    if (blockIdx.x == 0 && tid == 0) a.itoff[it] = (int)n_out;
     unsigned long long* pcur = a.pack + (size_t)p * a.L;
     KS_TRACE(it, 3, ks_globaltimer());
-    while (true) {
-      unsigned base = 0;
-      if (lane == 0) base = atomicAdd(&a.wctr[p], (unsigned)kGrab);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if ((long long)base >= n_items) break;
-      for (int g = 0; g < kGrab; ++g) {
-        const long long w = (long long)base + g;
-        if (w >= n_items) break;
-        if (w < n_upd) {
-          const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
-          const int r = (int)(w % rgroups);
-          const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
-          update_warp_item(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
-        } else {
-          const long long x = w - n_upd;
-          xres_warp_item(a, s, (int)(x / xgroups), (int)(x % xgroups), lane, warp);
-        }
-      }
+    // items of equal cost, dealt round-robin: consecutive items (neighbouring
+    // blocks, which share the slabs of their peaks) run concurrently
+    for (long long w = gwarp; w < n_items; w += nwarps) {
+      const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
+      const int r = (int)(w % rgroups);
+      const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
+      update_warp_item(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
     }
     KS_TRACE(it, 4, ks_globaltimer());
     KS_TRACE(it, 5, total);
@@ -630,6 +599,183 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
     a.info[1] = e ? e : status;
     a.info[2] = it;
     if (status != KS_ERR_OVERFLOW) a.info[3] = n_out;
+  }
+}
+
+struct ResSmem {
+  const float* W;  // P*nt
+  int* xl_tau;     // warps*kXList
+  int* xl_k;
+  float* xl_amp;
+};
+
+// ---------------------------------------------------------------- RESIDUAL
+// After the loop: Xres[c, col] -= amp_s * sum_p U[k_s,p,c] W[p, col-tau_s+nt/2]
+// for every spike s whose window covers col, applied in record order
+// (iteration, then time) -- per element the order in which the reference's
+// iterations subtract (:237).  Each element is read and written once.
+//
+// Gather, into the warp's list, the spikes of record positions
+// [skip, skip + kXList) among those whose window meets columns [c0, c0+32):
+// lanes binary-search the time-sorted run of one iteration each.  Returns the
+// total number of such spikes.
+__device__ int gather_residual(const PeelArgs& a, const ResSmem& s, int n_iter,
+                               long long n_out, int c0, int skip, int lane, int warp) {
+  __syncwarp();   // earlier readers of the warp's list are done
+  const int half = a.nt / 2;
+  const long long wlo = (long long)c0 - half, whi = (long long)c0 + kCol - 1 + half;
+  int* ltau = s.xl_tau + warp * kXList;
+  int* lk = s.xl_k + warp * kXList;
+  float* lamp = s.xl_amp + warp * kXList;
+  int total = 0;
+  for (int i0 = 0; i0 < n_iter; i0 += 32) {
+    const int i = i0 + lane;
+    long long first = 0, last = 0;
+    if (i < n_iter) {
+      long long lo = a.itoff[i];
+      const long long end = (i + 1 < n_iter) ? a.itoff[i + 1] : n_out;
+      long long hi = end;
+      while (lo < hi) {                       // first record with tau >= wlo
+        const long long mid = (lo + hi) >> 1;
+        if (a.st[2 * mid] < wlo) lo = mid + 1; else hi = mid;
+      }
+      first = lo;
+      last = lo;
+      while (last < end && a.st[2 * last] <= whi) ++last;
+    }
+    const int cnt = (int)(last - first);
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int base = total + incl - cnt;
+    for (int e = 0; e < cnt; ++e) {
+      const int pos = base + e - skip;
+      if (pos >= 0 && pos < kXList) {
+        const long long o = first + e;
+        ltau[pos] = (int)a.st[2 * o];
+        lk[pos] = (int)a.st[2 * o + 1];
+        lamp[pos] = a.amps[o];
+      }
+    }
+    total += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  __syncwarp();
+  return total;
+}
+
+// Load into the warp's list the spikes whose residual window meets block blk,
+// in record order.  Returns their number; when it exceeds kXCap the per-block
+// record list overflowed and the caller gathers with gather_residual instead.
+__device__ int load_residual_list(const PeelArgs& a, const ResSmem& s, int blk, int lane,
+                                  int warp) {
+  __syncwarp();
+  const int n = a.xcount[blk];
+  if (n > kXCap) return n;
+  const int o = lane < n ? a.xlist[(size_t)blk * kXCap + lane] : 0x7fffffff;
+  int rank = 0;
+  for (int j = 0; j < n; ++j) {
+    const int oj = __shfl_sync(0xffffffffu, o, j);
+    rank += (oj < o) ? 1 : 0;
+  }
+  if (lane < n) {
+    s.xl_tau[warp * kXList + rank] = (int)a.st[2 * (long long)o];
+    s.xl_k[warp * kXList + rank] = (int)a.st[2 * (long long)o + 1];
+    s.xl_amp[warp * kXList + rank] = a.amps[o];
+  }
+  __syncwarp();
+  return n;
+}
+
+// Residual of block blk for channels [32*cg, 32*cg + 32): lanes run over
+// channels, each lane keeps its 32 residual values in registers while the
+// listed spikes are subtracted in record order.
+__device__ void residual_item(const PeelArgs& a, const ResSmem& s, int n_iter, long long n_out,
+                              int blk, int cg, int lane, int warp) {
+  const int c0 = blk * kCol;
+  const int half = a.nt / 2, nt = a.nt, P = a.P;
+  const int c = cg * 32 + lane;
+  const bool chok = c < a.C;
+  int total = load_residual_list(a, s, blk, lane, warp);
+  const bool overflow = total > kXCap;
+  if (overflow) total = gather_residual(a, s, n_iter, n_out, c0, 0, lane, warp);
+  if (total == 0) return;
+  const int ncol = min(kCol, a.L - c0);
+  float* xrow = a.Xres + (long long)c * a.L + c0;
+  float x[kCol];
+#pragma unroll
+  for (int j = 0; j < kCol; ++j) x[j] = (chok && j < ncol) ? xrow[j] : 0.f;
+  const int epochs = (total + kXList - 1) / kXList;
+  for (int ep = 0; ep < epochs; ++ep) {
+    if (ep > 0) gather_residual(a, s, n_iter, n_out, c0, ep * kXList, lane, warp);
+    const int n = min(kXList, total - ep * kXList);
+    for (int e = 0; e < n; ++e) {
+      const int tau = s.xl_tau[warp * kXList + e];
+      const int k = s.xl_k[warp * kXList + e];
+      const float amp = s.xl_amp[warp * kXList + e];
+      float u[8];
+#pragma unroll
+      for (int pp = 0; pp < 8; ++pp)
+        u[pp] = (chok && pp < P) ? __ldg(a.U + ((long long)k * P + pp) * a.C + c) : 0.f;
+      const int t0 = c0 - tau + half;   // tap of column c0
+#pragma unroll
+      for (int j = 0; j < kCol; ++j) {
+        const int t = t0 + j;
+        if (t >= 0 && t < nt) {
+          float wv = 0.f;
+#pragma unroll
+          for (int pp = 0; pp < 8; ++pp)
+            if (pp < P) wv = fmaf(u[pp], s.W[pp * nt + t], wv);
+          x[j] = __fsub_rn(x[j], __fmul_rn(amp, wv));
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kCol; ++j)
+    if (chok && j < ncol) xrow[j] = x[j];
+}
+
+constexpr int kResThreads = 256;
+constexpr int kResWarps = kResThreads / 32;
+
+// One warp per (32-column block, 32 channels) of the residual; runs after the
+// peel kernel on the same stream and reads its outcome from info.
+__global__ void __launch_bounds__(kResThreads)
+ks_residual_kernel(PeelArgs a) {
+  extern __shared__ __align__(16) char smem_raw[];
+  float* sW = reinterpret_cast<float*>(smem_raw);
+  const int wn = (a.P * a.nt + 3) & ~3;
+  ResSmem s;
+  s.W = sW;
+  s.xl_tau = reinterpret_cast<int*>(sW + wn);
+  s.xl_k = s.xl_tau + kResWarps * kXList;
+  s.xl_amp = reinterpret_cast<float*>(s.xl_k + kResWarps * kXList);
+  for (int i = threadIdx.x; i < a.P * a.nt; i += kResThreads) sW[i] = a.W[i];
+  __syncthreads();
+  const long long n_out = a.info[0];
+  const int status = (int)a.info[1];
+  const int n_iter = (int)a.info[2];
+  if (status != KS_OK || n_out <= 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int xg = (a.C + 31) / 32;
+  const long long n_items = (long long)a.nblk * xg;
+  const long long w = (long long)blockIdx.x * kResWarps + warp;
+  if (w >= n_items) return;
+  residual_item(a, s, n_iter, n_out, (int)(w / xg), (int)(w % xg), lane, warp);
+}
+
+size_t residual_smem_bytes(int P, int nt) {
+  return sizeof(float) * (((size_t)P * nt + 3) & ~size_t(3)) +
+         (size_t)kResWarps * kXList * (2 * sizeof(int) + sizeof(float));
+}
+
+__global__ void ks_nm_pair_kernel(const float* __restrict__ nm, int K, float2* __restrict__ nmi) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < K; j += gridDim.x * blockDim.x) {
+    const float v = nm[j];
+    const bool normal = v >= 1.17549435e-38f && v <= 3.40282347e38f;
+    nmi[j] = make_float2(v, normal ? __frcp_rn(v) : __int_as_float(0x7fc00000));
   }
 }
 
@@ -678,8 +824,9 @@ struct PeelLayout {
 };
 
 // Workspace order: [ctl: bar(2) err(1) pad(1) wctr(2) pad(2)] [tcount 2*nblk]
-// [dbits 2*nwords] [pack 2*L] -- everything up to the end of pack[1] is
-// zeroed per launch -- then the settled scores, chunk buffers and touch lists.
+// [dbits 2*nwords] [xcount nblk] [pack 2*L] -- everything up to the end of
+// pack[1] is zeroed per launch -- then the settled scores, chunk buffers,
+// touch lists, iteration offsets and residual lists.
 PeelLayout peel_layout(int64_t L) {
   PeelLayout l;
   l.nchunks = (int)((L + kChunk - 1) / kChunk);
@@ -689,6 +836,7 @@ PeelLayout peel_layout(int64_t L) {
   cv.take<unsigned>(8);
   cv.take<int>(2 * (size_t)l.nblk);
   cv.take<unsigned>(2 * (size_t)l.nwords);
+  cv.take<int>(l.nblk);
   cv.take<unsigned long long>(2 * (size_t)L);
   l.zero_bytes = cv.used;
   cv.take<float>(L);
@@ -696,6 +844,9 @@ PeelLayout peel_layout(int64_t L) {
   cv.take<int>(l.nchunks);
   for (int i = 0; i < 4; ++i) cv.take<int>((size_t)l.nchunks * kChunk);
   cv.take<Touch>(2 * (size_t)l.nblk * kTouch);
+  cv.take<int>(kMaxIters);
+  cv.take<int>((size_t)l.nblk * kXCap);
+  cv.take<float2>(kMaxTemplates);
   l.bytes = cv.used;
   return l;
 }
@@ -744,10 +895,12 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
     return fail(KS_ERR_ARG, "ks_peel: null pointer");
   if (C < 1 || L < 1 || K < 1 || P < 1 || nt < 1 || (nt % 2) == 0)
     return fail(KS_ERR_ARG, "ks_peel: need C,L,K,P >= 1 and odd nt");
-  if (L > (int64_t)kMaxChunks * kChunk || K > (1 << 24) || C > (1 << 24) || nt > 1023 ||
+  if (L > (int64_t)kMaxChunks * kChunk || K > kMaxTemplates || C > (1 << 24) || nt > 1023 ||
       P > 8)
     return fail(KS_ERR_UNSUPPORTED, "ks_peel: shape beyond supported limits");
   if (capacity < 0 || max_peels < 0) return fail(KS_ERR_ARG, "ks_peel: negative capacity/max_peels");
+  if (max_peels > kMaxIters) return fail(KS_ERR_UNSUPPORTED, "ks_peel: max_peels above 4096");
+  if (capacity > 0x7fffffffLL) return fail(KS_ERR_UNSUPPORTED, "ks_peel: capacity above 2^31-1");
   if (!(th2 >= 0.f)) return fail(KS_ERR_ARG, "ks_peel: th2 must be a non-negative number");
   const PeelLayout lay = peel_layout(L);
   if (ws_bytes < lay.bytes || !ws) return fail(KS_ERR_WORKSPACE, "ks_peel: workspace too small");
@@ -760,7 +913,7 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
   a.Bt = Bt; a.Xres = Xres; a.U = U; a.W = W; a.ctcT = ctcT; a.nm = nm;
   a.C = (int)C; a.L = (int)L; a.K = (int)K; a.P = (int)P; a.nt = (int)nt;
   a.th2 = th2;
-  a.max_peels = (int)std::min<int64_t>(max_peels, 1 << 30);
+  a.max_peels = (int)max_peels;
   a.capacity = capacity;
   a.st = reinterpret_cast<long long*>(st); a.amps = amps; a.th_amps = th_amps;
   a.info = reinterpret_cast<long long*>(info);
@@ -771,6 +924,7 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
   a.wctr = ctl + 4;
   a.tcount = cv.take<int>(2 * (size_t)lay.nblk);
   a.dbits = cv.take<unsigned>(2 * (size_t)lay.nwords);
+  a.xcount = cv.take<int>(lay.nblk);
   a.pack = cv.take<unsigned long long>(2 * (size_t)L);
   a.cfmax = cv.take<float>(L);
   a.imax = cv.take<int>(L);
@@ -780,6 +934,10 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
   a.chunk_amp = cv.take<float>((size_t)lay.nchunks * kChunk);
   a.chunk_th = cv.take<float>((size_t)lay.nchunks * kChunk);
   a.touch = cv.take<Touch>(2 * (size_t)lay.nblk * kTouch);
+  a.itoff = cv.take<int>(kMaxIters);
+  a.xlist = cv.take<int>((size_t)lay.nblk * kXCap);
+  float2* nmi = cv.take<float2>(kMaxTemplates);
+  a.nmi = nmi;
   a.nchunks = lay.nchunks; a.nblk = lay.nblk; a.nwords = lay.nwords;
   a.limit_ns = limit_ns;
   a.upstream_err = upstream_err;
@@ -798,8 +956,15 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
   }
   const int grid = dev.sm_count * cached_occ;
   KS_CUDA(cudaMemsetAsync(ws, 0, lay.zero_bytes, stream));
+  ks_nm_pair_kernel<<<(unsigned)((K + 255) / 256), 256, 0, stream>>>(nm, (int)K, nmi);
+  KS_CUDA(cudaGetLastError());
   void* args[] = {&a};
   KS_CUDA(cudaLaunchCooperativeKernel((void*)peel_kernel, dim3(grid), dim3(kThreads), args, smem, stream));
+  // residual updates of all recorded spikes
+  const long long n_res = (long long)a.nblk * ((C + 31) / 32);
+  const unsigned rgrid = (unsigned)((n_res + kResWarps - 1) / kResWarps);
+  ks_residual_kernel<<<rgrid, kResThreads, residual_smem_bytes(a.P, a.nt), stream>>>(a);
+  KS_CUDA(cudaGetLastError());
   return KS_OK;
 }
 
