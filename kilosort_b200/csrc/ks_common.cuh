@@ -69,27 +69,26 @@ __device__ __forceinline__ int ks_ld_volatile(const int* p) {
   return *reinterpret_cast<const volatile int*>(p);
 }
 
-// Device-wide barrier for a cooperative (co-resident) grid.  bar[0] counts
-// arrivals, bar[1] is the generation.  A wait that exceeds limit_ns records
-// KS_ERR_TIMEOUT in *err and returns; every caller then sees the error flag
-// and leaves its loop, so no block waits without bound.
-// Returns true when no error is recorded.
-__device__ __forceinline__ bool ks_grid_sync(unsigned* bar, unsigned nblocks,
-                                             int* err,
+// Device-wide barrier for a cooperative (co-resident) grid.  *count starts
+// at zero and only grows: barrier number `epoch` (1, 2, ...) completes when it
+// reaches epoch * nblocks, so arriving is a single atomic and there is no reset
+// to order.  Every block passes the same sequence of barriers and keeps its own
+// epoch.  A wait that exceeds limit_ns records KS_ERR_TIMEOUT in *err and
+// returns; every caller then sees the error flag and leaves its loop, so no
+// block waits without bound.  Returns true when no error is recorded.
+__device__ __forceinline__ bool ks_grid_sync(unsigned* count, unsigned nblocks,
+                                             unsigned& epoch, int* err,
                                              unsigned long long limit_ns) {
   __syncthreads();
+  ++epoch;
   if (threadIdx.x == 0) {
-    unsigned gen = ks_ld_acquire(&bar[1]);
+    const unsigned target = epoch * nblocks;
     __threadfence();
-    unsigned arrived = atomicAdd(&bar[0], 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(&bar[0], 0u);
-      __threadfence();
-      atomicAdd(&bar[1], 1u);
-    } else {
-      unsigned long long t0 = ks_globaltimer();
-      while (ks_ld_acquire(&bar[1]) == gen) {
-        __nanosleep(64);
+    atomicAdd(count, 1u);
+    if (ks_ld_acquire(count) < target) {
+      const unsigned long long t0 = ks_globaltimer();
+      while (ks_ld_acquire(count) < target) {
+        __nanosleep(20);
         if (ks_globaltimer() - t0 > limit_ns) {
           atomicCAS(err, 0, KS_ERR_TIMEOUT);
           break;

@@ -32,7 +32,8 @@
 //   UPDATE  every block computes the exclusive prefix of the chunk counts (a
 //           peak's global index in the iteration) and of the dirty bitmap.
 //           Records are written in (iteration, tau) order.  Warps take work
-//           items round-robin: (dirty block in column order, row range):
+//           items (dirty block in column order, row range) round-robin, the
+//           last round from a counter:
 //           B[j,c] -= amp*ctc[j,k,c-tau+nt] for the peaks touching column c,
 //           even-indexed peaks first, then odd-indexed -- the order of the
 //           reference's two interleaved groups (:235-238) -- product and
@@ -71,9 +72,18 @@ constexpr int kXCap = 32;            // spikes recorded per block for the residu
     if (blockIdx.x == 0 && threadIdx.x == 0 && (it) < 200)               \
       a.info[8 + 8 * (it) + (slot)] = (long long)(value);                \
   } while (0)
+// every block's end-of-work stamp of iterations < 8 at info[1608 + it*G + block]
+#define KS_TRACE_CTA(it, value)                                                  \
+  do {                                                                           \
+    if (threadIdx.x == 0 && (it) < 8)                                            \
+      a.info[1608 + (it) * gridDim.x + blockIdx.x] = (long long)(value);          \
+  } while (0)
 #else
 #define KS_TRACE(it, slot, value) \
   do {                           \
+  } while (0)
+#define KS_TRACE_CTA(it, value) \
+  do {                          \
   } while (0)
 #endif
 
@@ -116,7 +126,7 @@ struct PeelArgs {
   int* itoff;                 // [kMaxIters] first record of each iteration
   int* xcount;                // [nblk] spikes whose residual window meets the block
   int* xlist;                 // [nblk * kXCap] their record indices (unordered)
-  unsigned* bar;              // {count, generation}
+  unsigned* bar;              // barrier arrival count (monotonic)
   int* err;
   const int* upstream_err;    // error word of the producer of Bt (may be null)
   int nchunks, nblk, nwords;
@@ -212,19 +222,12 @@ __device__ void detect_chunk(const PeelArgs& a, const Smem& s, int ch, int it) {
   const int wn = kChunk + 2 * nt;
   const int* tprev = a.tcount + (size_t)q * a.nblk;
   const unsigned long long* pprev = a.pack + (size_t)q * L;
-  if (it > 0) {
-    // nothing within +-nt of this chunk changed: its peak test cannot change
-    const int b_lo = max(a0 - nt, 0) / kCol, b_hi = min(a1 - 1 + nt, L - 1) / kCol;
-    int any = 0;
-    for (int b = b_lo + tid; b <= b_hi; b += kThreads) any |= tprev[b] > 0;
-    if (!__syncthreads_or(any)) {
-      if (tid == 0) a.chunk_cnt[ch] = 0;
-      return;
-    }
-  }
   // Column scores: rescored columns of the last iteration come from pack[q]
   // (and are settled into cfmax/imax by the chunk that owns them), the others
-  // from cfmax.  The candidate loads are independent and issued together.
+  // from cfmax.  The candidate loads are independent and issued together; if
+  // nothing within +-nt of the chunk changed, its peak test cannot change and
+  // the chunk is skipped.
+  int any_fresh = 0;
   for (int i = tid; i < wn; i += kThreads) {
     const int col = a0 - nt + i;
     float v;
@@ -238,6 +241,7 @@ __device__ void detect_chunk(const PeelArgs& a, const Smem& s, int ch, int it) {
       const float cv = a.cfmax[col];
       const bool own = i >= nt && i < nt + kChunk && col < a1;
       const int iv = own ? a.imax[col] : 0;
+      any_fresh |= fresh;
       v = fresh ? pack_value(pv) : cv;
       if (own) {
         const int kb = fresh ? pack_index(pv) : iv;
@@ -250,7 +254,10 @@ __device__ void detect_chunk(const PeelArgs& a, const Smem& s, int ch, int it) {
     }
     s.win[i] = v;
   }
-  __syncthreads();
+  if (!__syncthreads_or(any_fresh)) {
+    if (tid == 0) a.chunk_cnt[ch] = 0;
+    return;
+  }
   // sliding max over 2nt+1 columns: doubling levels up to the largest power
   // of two m <= 2nt+1, then the union of two overlapping m-windows
   const int len = 2 * nt + 1;
@@ -322,46 +329,56 @@ __device__ void detect_chunk(const PeelArgs& a, const Smem& s, int ch, int it) {
   __syncthreads();
 }
 
-// Exclusive prefix of n counts (read through get(i)) into out[0..n]; returns
-// the total.  All threads of the block take part.
-template <typename Get>
-__device__ int block_prefix(int n, Get get, int* out, int* wcnt) {
+// Both exclusive prefixes an iteration needs, in one pass: of the chunk peak
+// counts into s.prefix[0..nchunks] and of the dirty-bitmap word popcounts into
+// s.wprefix[0..nwords].  All threads of the block take part.
+__device__ void two_prefix(const int* cnt, int nchunks, const unsigned* bits, int nwords,
+                           const Smem& s, int& total, int& ndirty) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int per = (n + kThreads - 1) / kThreads;
-  const int c0 = tid * per;
-  int local = 0;
-  for (int i = 0; i < per; ++i) {
-    const int c = c0 + i;
-    if (c < n) local += get(c);
+  const int pc = (nchunks + kThreads - 1) / kThreads;
+  const int pw = (nwords + kThreads - 1) / kThreads;
+  int lc = 0, lw = 0;
+  for (int i = 0; i < pc; ++i) {
+    const int c = tid * pc + i;
+    if (c < nchunks) lc += cnt[c];
   }
-  int incl = local;
+  for (int i = 0; i < pw; ++i) {
+    const int w = tid * pw + i;
+    if (w < nwords) lw += __popc(bits[w]);
+  }
+  int ic = lc, iw = lw;
   for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
+    const int vc = __shfl_up_sync(0xffffffffu, ic, o);
+    const int vw = __shfl_up_sync(0xffffffffu, iw, o);
+    if (lane >= o) { ic += vc; iw += vw; }
   }
-  if (lane == 31) wcnt[warp] = incl;
+  int* wc = s.wcnt;                 // [kWarps+1] chunk totals per warp
+  int* ww = s.kidx;                 // [kWarps+1] word totals per warp (kidx is free here)
+  if (lane == 31) { wc[warp] = ic; ww[warp] = iw; }
   __syncthreads();
   if (tid == 0) {
-    int acc = 0;
+    int ac = 0, aw = 0;
     for (int w = 0; w < kWarps; ++w) {
-      const int c = wcnt[w];
-      wcnt[w] = acc;
-      acc += c;
+      const int c = wc[w], x = ww[w];
+      wc[w] = ac; ww[w] = aw;
+      ac += c; aw += x;
     }
-    wcnt[kWarps] = acc;
+    wc[kWarps] = ac; ww[kWarps] = aw;
   }
   __syncthreads();
-  int run = wcnt[warp] + incl - local;
-  for (int i = 0; i < per; ++i) {
-    const int c = c0 + i;
-    if (c < n) {
-      out[c] = run;
-      run += get(c);
-    }
+  int rc = wc[warp] + ic - lc, rw = ww[warp] + iw - lw;
+  for (int i = 0; i < pc; ++i) {
+    const int c = tid * pc + i;
+    if (c < nchunks) { s.prefix[c] = rc; rc += cnt[c]; }
   }
-  if (tid == 0) out[n] = wcnt[kWarps];
+  for (int i = 0; i < pw; ++i) {
+    const int w = tid * pw + i;
+    if (w < nwords) { s.wprefix[w] = rw; rw += __popc(bits[w]); }
+  }
+  if (tid == 0) { s.prefix[nchunks] = wc[kWarps]; s.wprefix[nwords] = ww[kWarps]; }
   __syncthreads();
-  return out[n];
+  total = s.prefix[nchunks];
+  ndirty = s.wprefix[nwords];
 }
 
 // ---------------------------------------------------------------- UPDATE
@@ -520,26 +537,25 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
   int it = 0;
   int status = KS_OK;
   KS_TRACE(0, 7, ks_globaltimer());
-  bool ok = ks_grid_sync(a.bar, G, a.err, a.limit_ns);
+  unsigned epoch = 0;
+  bool ok = ks_grid_sync(a.bar, G, epoch, a.err, a.limit_ns);
   for (; ok && it < a.max_peels; ++it) {
     const int p = it & 1, q = p ^ 1;
     KS_TRACE(it, 0, ks_globaltimer());
     for (int ch = blockIdx.x; ch < a.nchunks; ch += G) detect_chunk(a, s, ch, it);
     KS_TRACE(it, 1, ks_globaltimer());
-    if (!ks_grid_sync(a.bar, G, a.err, a.limit_ns)) break;
+    if (!ks_grid_sync(a.bar, G, epoch, a.err, a.limit_ns)) break;
     KS_TRACE(it, 2, ks_globaltimer());
 
-    const int* cnt = a.chunk_cnt;
-    const int total = block_prefix(a.nchunks, [cnt](int i) { return cnt[i]; }, s.prefix, s.wcnt);
+    const unsigned* bits = a.dbits + (size_t)p * a.nwords;
+    int total, ndirty;
+    two_prefix(a.chunk_cnt, a.nchunks, bits, a.nwords, s, total, ndirty);
     if (total == 0) break;
     if (n_out + total > a.capacity) {
       status = KS_ERR_OVERFLOW;
       if (blockIdx.x == 0 && tid == 0) a.info[3] = n_out + total;
       break;
     }
-    const unsigned* bits = a.dbits + (size_t)p * a.nwords;
-    const int ndirty = block_prefix(a.nwords, [bits](int i) { return __popc(bits[i]); },
-                                    s.wprefix, s.wcnt);
     for (int ch = blockIdx.x; ch < a.nchunks; ch += G) {
       const int c_n = a.chunk_cnt[ch];
       for (int i = tid; i < c_n; i += kThreads) {
@@ -566,12 +582,20 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
     if (blockIdx.x == 0 && tid == 0) a.wctr[q] = 0u;
     // update items: (dirty block in column order, row range), sized so that
     // there are about four per warp
+    // rows per item: the split whose most loaded warp has the least work
+    // (row groups of 16 plus one group's worth of per-item set-up)
     int rows = kItemRows;
     if (ndirty > 0) {
-      const long long per_blk = (4 * nwarps + ndirty - 1) / ndirty;   // items wanted per block
-      int r = (int)((a.K + per_blk - 1) / per_blk);
-      r = (r + kRowsPerWarp - 1) / kRowsPerWarp * kRowsPerWarp;   // whole row groups
-      rows = max(kRowsPerWarp, min(kItemRows, r));
+      long long best_cost = -1;
+      for (int r = kRowsPerWarp; r <= kItemRows; r += kRowsPerWarp) {
+        const long long items = (long long)ndirty * ((a.K + r - 1) / r);
+        const long long per_warp = (items + nwarps - 1) / nwarps;
+        const long long cost = per_warp * (r / kRowsPerWarp + 1);
+        if (best_cost < 0 || cost < best_cost) {
+          best_cost = cost;
+          rows = r;
+        }
+      }
     }
     const int rgroups = (a.K + rows - 1) / rows;
     const long long n_upd = (long long)ndirty * rgroups;
@@ -579,19 +603,35 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
     if (blockIdx.x == 0 && tid == 0) a.itoff[it] = (int)n_out;
     unsigned long long* pcur = a.pack + (size_t)p * a.L;
     KS_TRACE(it, 3, ks_globaltimer());
-    // items of equal cost, dealt round-robin: consecutive items (neighbouring
-    // blocks, which share the slabs of their peaks) run concurrently
-    for (long long w = gwarp; w < n_items; w += nwarps) {
+    // Items of equal cost.  All but the last round are dealt round-robin
+    // (consecutive items -- neighbouring blocks, which share the slabs of their
+    // peaks -- run concurrently); the rest go to whichever warp asks first, so
+    // warps that ran into slower memory take fewer of them.
+    const long long rounds = n_items / nwarps;
+    const long long n_static = rounds > 1 ? (rounds - 1) * nwarps : 0;
+    for (long long w = gwarp; w < n_static; w += nwarps) {
+      const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
+      const int r = (int)(w % rgroups);
+      const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
+      update_warp_item(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
+    }
+    while (true) {
+      unsigned next = 0;
+      if (lane == 0) next = atomicAdd(&a.wctr[p], 1u);
+      const long long w = n_static + (long long)__shfl_sync(0xffffffffu, next, 0);
+      if (w >= n_items) break;
       const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
       const int r = (int)(w % rgroups);
       const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
       update_warp_item(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
     }
     KS_TRACE(it, 4, ks_globaltimer());
+    __syncthreads();
+    KS_TRACE_CTA(it, ks_globaltimer());
     KS_TRACE(it, 5, total);
     KS_TRACE(it, 6, ndirty);
     n_out += total;
-    ok = ks_grid_sync(a.bar, G, a.err, a.limit_ns);
+    ok = ks_grid_sync(a.bar, G, epoch, a.err, a.limit_ns);
   }
   if (blockIdx.x == 0 && tid == 0) {
     const int e = ks_ld_volatile(a.err);
