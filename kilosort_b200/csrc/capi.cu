@@ -86,7 +86,7 @@ static MatchLayout match_layout(int64_t C, int64_t L, int64_t K, int64_t P, int6
   m.ctc_off = off;
   off += ctcT_bytes(K, nt, ctc_layout);
   m.peel_off = off;
-  off = align256(off + peel_scratch_size(L));
+  off = align256(off + peel_scratch_size(L, K));
   m.bytes = off;
   return m;
 }
@@ -105,7 +105,7 @@ static PeelWsLayout peel_ws_layout(int64_t L, int64_t K, int64_t nt, int b_layou
   m.ctc_off = off;
   off += ctcT_bytes(K, nt, ctc_layout);
   m.peel_off = off;
-  off = align256(off + peel_scratch_size(L));
+  off = align256(off + peel_scratch_size(L, K));
   m.bytes = off;
   return m;
 }

@@ -70,7 +70,7 @@ extern "C" KS_API int ks_peel_static(float* Bt, float* Xres, const float* U, con
     return fail(KS_ERR_UNSUPPORTED,
                 "ks_peel_static: batch length must be 1.." + std::to_string(KS_PEEL_STATIC_MAX_L) +
                     " padded samples (the fixed scratch array is sized for that)");
-  const size_t need = peel_scratch_size(L);
+  const size_t need = peel_scratch_size(L, K);
   if (need > kPeelStaticBytes)
     return fail(KS_ERR_UNSUPPORTED, "ks_peel_static: scratch for this batch exceeds the fixed array");
   DeviceInfo dev;

@@ -35,7 +35,7 @@ int gemm_bf16x3(const __nv_bfloat16* Uhi, const __nv_bfloat16* Ulo,
 
 // Peel on a tiled score matrix Bt [ceil(L/32)][K][32] and a transposed
 // cross-correlation ctcT[k][j][lag] = ctc[j][k][lag].
-size_t peel_scratch_size(int64_t L);
+size_t peel_scratch_size(int64_t L, int64_t K);
 int64_t tiled_rows_floats(int64_t L, int64_t K);
 int launch_tile_rows(const float* B, int64_t ldb, int64_t K, int64_t L, float* Bt,
                      cudaStream_t stream);
