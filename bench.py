@@ -36,6 +36,9 @@ NT = 61
 N_PCS = 6
 TH = 8.0
 CFG = 2
+# DRAM bytes (read + write) of one peel_kernel launch on a C=384/K=600/60000-sample
+# batch, from the ncu capture summarised in profiles/peel_kernel_c384_k600.txt
+PEEL_TRAFFIC_BYTES = 8.709e9
 WORKLOAD = ("Neuropixels-scale matching: C=384 (NP1-like), K=600 templates, 20 batches x "
             "60000 samples (+2*61 pad), nt=61, n_pcs=6, Th_learned=8, max_peels=100")
 
@@ -48,6 +51,11 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batches", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="np1", choices=["np1", "uneven"],
+                   help="np1: C=384/K=600, 20 equal batches (default); uneven: three "
+                        "recordings, 200 batches of uneven length, batched launches")
+    p.add_argument("--group", type=int, default=50,
+                   help="uneven workload: batches per batched call (one graph each)")
     return p.parse_args()
 
 
@@ -156,6 +164,101 @@ def reference_arm(args, rank):
     }
     print(json.dumps(line), flush=True)
 
+UNEVEN = ("three recordings (C/K = 96/150, 384/600, 384/1000), 200 padded batches with "
+          "NT_b ~ U[8000, 60000] and a short tail batch each, nt=61, n_pcs=6, Th_learned=8, "
+          "max_peels=100, split-BF16 projection")
+
+
+def uneven_main(args, dev, rank, world):
+    """Batched form: every batch of three recordings through ks_match_batches.
+
+    A step is one pass over all batches: groups of --group batches, each a
+    captured CUDA graph (grouped projection, one cooperative peel launch split
+    into autotuned teams, one residual launch).  The same batches through one
+    run_matching call each are timed beside it.  X resident in HBM.
+    """
+    import kilosort_b200 as kb
+    from kilosort_b200 import synth
+    from kilosort_b200.batched import (BatchedMatcher, Recording, autotune_teams,
+                                       workspace_size)
+    recs = synth.uneven_recordings(seed=1003, n_batches_total=200)
+    mrecs, items, ops_l = [], [], []
+    for i, r in enumerate(recs):
+        U = torch.from_numpy(r.U).to(dev)
+        W = torch.from_numpy(r.wPCA).to(dev)
+        ops = dict(Th_learned=TH, nt=r.nt, max_peels=100, wPCA=W)
+        ctc = kb.prepare_matching(ops, U)
+        mrecs.append(Recording.from_ops(ops, U, ctc))
+        ops_l.append((ops, U, ctc))
+        for b in range(r.n_batches):
+            items.append((torch.from_numpy(np.ascontiguousarray(r.batch(b))).to(dev), i))
+    # interleave recordings: groups mix template sets and lengths
+    order = sorted(range(len(items)), key=lambda i: (i * 7919) % len(items))
+    items = [items[i] for i in order]
+    groups = [items[g:g + args.group] for g in range(0, len(items), args.group)]
+    samples = sum(recs[r].n_chan * (X.shape[1] - 2 * recs[r].nt) for X, r in items)
+    teams = autotune_teams(mrecs, groups[0], "bf16x3", candidates=(2, 4, 8, 12, 16, 24))
+    # the groups run one after the other on one stream: one shared workspace
+    ws = torch.empty(max(workspace_size(mrecs, g, "bf16x3", teams) for g in groups),
+                     dtype=torch.uint8, device=dev)
+    matchers = [BatchedMatcher(mrecs, [(X.shape[1], r) for X, r in g], "bf16x3", teams=teams,
+                               graph=True, workspace=ws) for g in groups]
+    for m, g in zip(matchers, groups):
+        for dst, (X, _) in zip(m.X, g):
+            dst.copy_(X)
+
+    def batched_step():
+        for m in matchers:
+            m.launch()
+
+    def loop_step():
+        for X, r in items:
+            ops, U, ctc = ops_l[r]
+            kb.run_matching(dict(ops, projection="bf16x3"), X, U, ctc, device=dev)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    sampler = ClockSampler(dev.index or 0)
+    for _ in range(args.warmup):
+        batched_step()
+    torch.cuda.synchronize()
+    nsp = sum(len(r[0]) for m in matchers for r in m.results())
+    sampler.__enter__()
+    ms = timed(batched_step)
+    sampler.__exit__()
+    ms_loop = timed(loop_step)
+    value = samples * world / (ms * 1e-3)
+    line = {
+        "metric": "channel-samples/s", "value": value, "unit": "channel-samples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (split-bf16 projection)", "data": "synthetic",
+        "config": {"workload": UNEVEN, "batches": len(items), "group": args.group,
+                   "teams": teams, "graphs": len(matchers),
+                   "l2": f"inputs larger than L2 ({sum(X.numel() for X, _ in items) * 4 / 1e9:.1f}"
+                         " GB of X per step)", "parallelism": f"replicas x{world}"},
+        "spikes_per_step": nsp,
+        "per_batch_run_matching": {"ms_per_step": ms_loop,
+                                   "channel_samples_per_s": samples * world / (ms_loop * 1e-3)},
+        "speedup_batched_vs_per_batch": ms_loop / ms,
+        "clocks": sampler.summary(),
+        # per group: energy, {nm, 1/nm}, reorder per recording; temporal per
+        # batch; grouped contraction, peel, residual
+        "gpu_launches": sum(3 * len(mrecs) + len(m.items) + 3 for m in matchers),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
 
 def main():
     args = parse()
@@ -173,6 +276,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
 
+    if args.workload == "uneven":
+        uneven_main(args, dev, rank, world)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     import kilosort_b200 as kb
     from kilosort_b200 import _lib, synth
     from tests.parity_util import agreement
@@ -260,44 +368,53 @@ def main():
 
     e2e_ms, _ = timed(e2e_step, head)
 
-    # stage breakdown of one pass with the kernels run_matching launches
-    # (projection into the tiled score layout, then the peel), device-timed:
-    # no host synchronisation inside either bracket
-    stage = {"project": 0.0, "peel": 0.0}
-    stage_batches = {"project": [], "peel": []}
+    # per-kernel breakdown of one pass through the public run_matching, timed
+    # by events the library records inside the call (ks_trace_stages): energy
+    # + copy, projection, peel kernel, residual kernel; one warm-up pass first
+    lib = _lib.load()
+    _lib.check(lib.ks_trace_stages(1), "ks_trace_stages")
+    import ctypes
+    ms4 = (ctypes.c_float * 4)()
+    stage = {"energy": 0.0, "project": 0.0, "peel": 0.0, "residual": 0.0}
+    stage_batches = {k: [] for k in stage}
     kused, nsp_total = 0, 0
-    nm = kb.template_energy(U)
-    ctcT = kb.transpose_ctc(ctc, NT)
-    Bt = kb.project_scores(Xs[0], U, W, NT, head, tiled=True)
-    for X in Xs:
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        Xres = X.clone()
-        torch.cuda.synchronize()
-        e[0].record()
-        Bt = kb.project_scores(X, U, W, NT, head, tiled=True, check_status=False)
-        e[1].record()
-        st, amps, th, _ = kb.peel(Bt, Xres, U, W, ctcT, nm, TH, NT, 100, ctc_transposed=True)
-        e[2].record()
-        torch.cuda.synchronize()
-        tp, tq = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
-        stage["project"] += tp
-        stage["peel"] += tq
-        stage_batches["project"].append(round(tp, 3))
-        stage_batches["peel"].append(round(tq, 3))
-        kused += len(torch.unique(st[:, 1]))
-        nsp_total += len(st)
+    o_head = dict(ops, projection=head)
+    for pass_ in range(2):
+        for X in Xs:
+            st, amps, th, _ = kb.run_matching(o_head, X, U, ctc, device=dev)
+            _lib.check(lib.ks_trace_read(ms4, 4), "ks_trace_read")
+            if pass_ == 0:
+                continue
+            for key, v in zip(stage, ms4):
+                stage[key] += v
+                stage_batches[key].append(round(v, 3))
+            kused += len(torch.unique(st[:, 1]))
+            nsp_total += len(st)
+    _lib.check(lib.ks_trace_stages(0), "ks_trace_stages")
     nb = args.batches
     hbm, bf16, peak_kind = peaks()
     flop_proj = 2.0 * L * C * N_PCS * (NT + K) * nb
-    bytes_peel = (4.0 * K * L + 8.0 * C * L) * nb + 4.0 * K * (2 * NT + 1) * kused \
+    # compulsory bytes of the peel (B read once, X/Xres, ctc columns and
+    # loadings of the templates used, outputs) and the no-reuse bound (every
+    # spike's K x (2nt+1) read-modify-write of B plus its ctc column, and its
+    # C x nt residual update)
+    bytes_peel = 4.0 * K * L * nb + 4.0 * K * (2 * NT + 1) * kused \
         + 4.0 * N_PCS * C * kused + 24.0 * nsp_total
+    bytes_res = 8.0 * C * L * nb
+    bytes_noreuse = 4.0 * K * L * nb + nsp_total * (12.0 * K * (2 * NT + 1) + 8.0 * C * NT)
     proj_tflops = flop_proj / (stage["project"] * 1e-3) / 1e12
     peel_gbs = bytes_peel / (stage["peel"] * 1e-3) / 1e9
     fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+    traffic = PEEL_TRAFFIC_BYTES if (C, K, NT_BATCH) == (384, 600, 60000) else None
     if stage["peel"] >= stage["project"]:
-        roof = {"kernel": "peel", "bound": "hbm", "achieved": peel_gbs, "peak": hbm,
-                "unit": "GB/s", "frac": peel_gbs / hbm, "traffic": None,
-                "peak_source": peak_kind}
+        roof = {"kernel": "peel_kernel", "bound": "hbm", "achieved": peel_gbs, "peak": hbm,
+                "unit": "GB/s", "frac": peel_gbs / hbm, "traffic": traffic,
+                "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": bytes_peel / nb,
+                "no_reuse_bytes_per_launch": bytes_noreuse / nb,
+                "traffic_gbs": (traffic / (stage["peel"] / nb * 1e-3) / 1e9
+                                if traffic else None),
+                "ms_per_launch": stage["peel"] / nb}
     elif head == "bf16x3":
         roof = {"kernel": "project_bf16x3", "bound": "tensor", "achieved": proj_tflops,
                 "peak": bf16, "unit": "TFLOP/s", "frac": proj_tflops / bf16, "traffic": None,
@@ -319,7 +436,8 @@ def main():
             a = agreement(st.cpu().numpy(), st_r, amps.cpu().numpy(), amps_r)
             agr[form] = {k: a[k] for k in ("agreement", "amp_rel_max", "matched", "n_a", "n_r")}
 
-    launches_per_batch = 5  # energy, reorder, temporal, contraction, peel
+    # energy, reorder, temporal, contraction, {nm, 1/nm}, peel, residual
+    launches_per_batch = 7
     per_step_samples = C * NT_BATCH * nb
     head_ms = results[head]["ms"]
     value = per_step_samples * world / (head_ms * 1e-3)
@@ -345,8 +463,11 @@ def main():
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h[0],
                 "ms_per_step": e2e_ms},
         "roofline": roof,
-        "roofline_all": {"project": {"achieved_tflops": proj_tflops},
-                         "peel": {"achieved_gbs": peel_gbs, "algorithmic_bytes": bytes_peel}},
+        "roofline_all": {"project": {"achieved_tflops": proj_tflops,
+                                     "flop_per_batch": flop_proj / nb},
+                         "peel": {"achieved_gbs": peel_gbs, "algorithmic_bytes": bytes_peel},
+                         "residual": {"achieved_gbs": bytes_res / (stage["residual"] * 1e-3) / 1e9,
+                                      "algorithmic_bytes": bytes_res}},
         "cpu_baseline": cpu,
         "clocks": sampler.summary(),
         "gpu_launches": launches_per_batch * nb,

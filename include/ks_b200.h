@@ -181,6 +181,70 @@ KS_API int ks_peel_static(float* Bt, float* Xres, const float* U, const float* W
                           float* amps, float* th_amps, int64_t* info, void* stream);
 
 /*
+ * Many batches of several recordings in a few launches.
+ * Replaces the per-batch loop of kilosort/template_matching.py:79-84
+ * (extract: padded_batch_to_torch, then run_matching per batch), for up to
+ * KS_MAX_BATCHES batches of up to KS_MAX_RECORDINGS recordings (template sets)
+ * per call; batch lengths may differ.  Each batch gets exactly the outputs
+ * ks_run_matching gives it (st, amps, th_amps, Xres, info), computed in this
+ * order on the stream: per recording the template energies and the reordered
+ * templates; per batch Xres = X and the temporal projection; the score
+ * contraction of every batch (split-BF16: one grouped tensor-core launch;
+ * FP32: one launch per batch); one cooperative peel launch whose grid is split
+ * into `teams` groups of co-resident blocks, each peeling its share of the
+ * batches (longest first) with no host round trip; one residual launch for all
+ * batches.  teams <= 0 picks a default.  info[1] of a batch that no team
+ * reached (after an error) stays -1.  Nothing is copied from host memory and
+ * the host is not synchronised, so the call can be captured in a CUDA graph
+ * (the descriptors are read at call time).  ctcT is the transposed layout
+ * (KS_CTC_KJL).  Xres may equal X (in place); otherwise they must not overlap.
+ */
+#define KS_MAX_BATCHES 256
+#define KS_MAX_RECORDINGS 8
+typedef struct ks_rec_desc {
+  const float* U;          /* [K, P, C] */
+  const float* W;          /* [P, nt]   wPCA */
+  const float* ctcT;       /* [K, K, 2*nt+1] transposed cross-correlations */
+  int64_t C, K, P, nt;
+  float th2;               /* float(Th_learned**2) */
+  int64_t max_peels;
+  int64_t capacity;        /* spike rows of each batch's outputs */
+} ks_rec_desc;
+typedef struct ks_batch_desc {
+  const float* X;          /* [C, L] */
+  float* Xres;             /* [C, L] */
+  int64_t L;
+  int64_t rec;             /* index into the recording descriptors */
+  int64_t* st;             /* [capacity, 2] */
+  float* amps;             /* [capacity] */
+  float* th_amps;          /* [capacity] */
+  int64_t* info;           /* [4] */
+} ks_batch_desc;
+KS_API size_t ks_match_batches_workspace_size(const ks_rec_desc* recs, int64_t n_recs,
+                                              const ks_batch_desc* batches,
+                                              int64_t n_batches, int precision,
+                                              int64_t teams);
+KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
+                            const ks_batch_desc* batches, int64_t n_batches,
+                            int precision, int64_t teams, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
+/*
+ * Stage timing of ks_run_matching, for profiling the public call as it runs
+ * (no work is skipped or added).  While enabled on the calling host thread,
+ * ks_run_matching records CUDA events at five points on its stream: start,
+ * after the template energies, after the projection, after the peel kernel,
+ * after the residual kernel.  ks_trace_read waits for the last of the first
+ * n+1 events of the thread's most recent traced call and writes n <= 4
+ * intervals in ms: [energy + copy, projection, peel kernel, residual].  The
+ * events are the library's, created on the current device by the first
+ * ks_trace_stages(1).  No reference counterpart (the reference has no
+ * tracing of this path).
+ */
+KS_API int ks_trace_stages(int enable);
+KS_API int ks_trace_read(float* ms, int n);
+
+/*
  * Watchdog self-test: one thread waits on a device flag that nothing sets,
  * bounded by timeout_ns, and writes KS_ERR_TIMEOUT to status[0] when the wait
  * runs out.  status points to two device ints (status[1] is the flag, cleared

@@ -60,7 +60,27 @@ SIGNATURES = {
     "ks_selftest_wait": (_int, [_i64, _vp, _vp]),
     "ks_peel_static": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
                               _f32, _i64, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "ks_trace_stages": (_int, [_int]),
+    "ks_trace_read": (_int, [_vp, _int]),
+    "ks_match_batches_workspace_size": (_sz, [_vp, _i64, _vp, _i64, _int, _i64]),
+    "ks_match_batches": (_int, [_vp, _i64, _vp, _i64, _int, _i64, _vp, _sz, _vp]),
 }
+
+KS_MAX_BATCHES = 256
+KS_MAX_RECORDINGS = 8
+
+
+class RecDesc(C.Structure):
+    """``ks_rec_desc``: one recording's template set and peel settings."""
+    _fields_ = [("U", _vp), ("W", _vp), ("ctcT", _vp), ("C", _i64), ("K", _i64),
+                ("P", _i64), ("nt", _i64), ("th2", _f32), ("max_peels", _i64),
+                ("capacity", _i64)]
+
+
+class BatchDesc(C.Structure):
+    """``ks_batch_desc``: one padded batch, its recording and its outputs."""
+    _fields_ = [("X", _vp), ("Xres", _vp), ("L", _i64), ("rec", _i64), ("st", _vp),
+                ("amps", _vp), ("th_amps", _vp), ("info", _vp)]
 
 _lib = None
 

@@ -1,0 +1,308 @@
+"""Many batches of several recordings per launch sequence (``ks_match_batches``).
+
+The reference matches one padded batch per ``run_matching`` call
+(kilosort/template_matching.py:79-84, the loop of ``extract``).  Here a whole
+group of batches -- up to 256, of up to 8 recordings (template sets), of any
+lengths -- goes through one grouped tensor-core contraction, one cooperative
+peel launch whose grid is split into teams of co-resident blocks, and one
+residual launch.  Each batch gets exactly what ``run_matching`` returns for it.
+
+* ``Recording``      one template set: U, wPCA, ctc (transposed once), Th, nt,
+                     max_peels, spike capacity per batch
+* ``match_batches``  one call over a list of ``(X, recording index)``
+* ``BatchedMatcher`` fixed shapes: preallocated inputs, outputs and workspace,
+                     optionally captured once in a CUDA graph and replayed
+* ``autotune_teams`` times candidate team counts on the device and caches the
+                     fastest per workload signature
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import torch
+
+from . import _lib
+from .template_matching import (DEFAULT_CAPACITY, _PROJECTIONS, _need, _ptr, _stream,
+                                th2_of, transpose_ctc)
+
+
+@dataclass
+class Recording:
+    """A template set and its peel settings (one ``ks_rec_desc``)."""
+
+    U: torch.Tensor
+    wPCA: torch.Tensor
+    ctc: torch.Tensor
+    Th: float
+    nt: int
+    max_peels: int = 100
+    capacity: int = DEFAULT_CAPACITY
+    ctcT: Optional[torch.Tensor] = field(default=None, repr=False)
+
+    def __post_init__(self):
+        self.U = _need(self.U, "U", ndim=3)
+        self.wPCA = _need(self.wPCA, "wPCA", ndim=2)
+        self.ctc = _need(self.ctc, "ctc", ndim=3)
+        K, P, _ = self.U.shape
+        if self.wPCA.shape != (P, self.nt):
+            raise ValueError(f"wPCA must be [{P}, {self.nt}], got {tuple(self.wPCA.shape)}")
+        if self.ctc.shape != (K, K, 2 * self.nt + 1):
+            raise ValueError("shape mismatch between U and ctc")
+        if self.ctcT is None:
+            self.ctcT = transpose_ctc(self.ctc, self.nt)
+
+    @classmethod
+    def from_ops(cls, ops, U, ctc, capacity=None):
+        cap = int(ops.get("spike_capacity", DEFAULT_CAPACITY)) if capacity is None else capacity
+        return cls(U=U, wPCA=ops["wPCA"], ctc=ctc, Th=ops["Th_learned"], nt=int(ops["nt"]),
+                   max_peels=int(ops["max_peels"]), capacity=cap)
+
+    @property
+    def shape(self):
+        K, P, Cn = self.U.shape
+        return Cn, K, P
+
+    def desc(self) -> _lib.RecDesc:
+        Cn, K, P = self.shape
+        return _lib.RecDesc(_ptr(self.U), _ptr(self.wPCA), _ptr(self.ctcT), Cn, K, P, self.nt,
+                            th2_of(self.Th), int(self.max_peels), int(self.capacity))
+
+
+class _Outputs:
+    """Device outputs of one batch."""
+
+    def __init__(self, rec: Recording, Cn: int, L: int, device, Xres=None):
+        cap = int(rec.capacity)
+        self.st = torch.empty((cap, 2), dtype=torch.int64, device=device)
+        self.amps = torch.empty((cap, 1), dtype=torch.float32, device=device)
+        self.th_amps = torch.empty((cap, 1), dtype=torch.float32, device=device)
+        self.Xres = torch.empty((Cn, L), dtype=torch.float32, device=device) if Xres is None else Xres
+
+
+def _check_group(recs: Sequence[Recording], items: Sequence[Tuple[torch.Tensor, int]]):
+    if not 1 <= len(recs) <= _lib.KS_MAX_RECORDINGS:
+        raise ValueError(f"1..{_lib.KS_MAX_RECORDINGS} recordings per call")
+    if not 1 <= len(items) <= _lib.KS_MAX_BATCHES:
+        raise ValueError(f"1..{_lib.KS_MAX_BATCHES} batches per call")
+    dev = recs[0].U.device
+    for X, r in items:
+        if not 0 <= r < len(recs):
+            raise ValueError(f"recording index {r} out of range")
+        X = _need(X, "X", ndim=2)
+        if X.shape[0] != recs[r].shape[0]:
+            raise ValueError(f"batch has {X.shape[0]} channels, recording {r} has {recs[r].shape[0]}")
+        if X.device != dev:
+            raise ValueError("all tensors must be on one device")
+    return dev
+
+
+def _descs(recs, items, outs, info):
+    rd = (_lib.RecDesc * len(recs))(*[r.desc() for r in recs])
+    bd = (_lib.BatchDesc * len(items))()
+    for i, ((X, r), o) in enumerate(zip(items, outs)):
+        bd[i] = _lib.BatchDesc(_ptr(X), _ptr(o.Xres), X.shape[1], r, _ptr(o.st), _ptr(o.amps),
+                               _ptr(o.th_amps), _ptr(info[i]))
+    return rd, bd
+
+
+def workspace_size(recs, items, projection="bf16x3", teams=0) -> int:
+    rd = (_lib.RecDesc * len(recs))(*[r.desc() for r in recs])
+    bd = (_lib.BatchDesc * len(items))()
+    for i, (X, r) in enumerate(items):
+        # pointers are not read by the size query; shapes are
+        bd[i] = _lib.BatchDesc(1, 1, X.shape[1], r, 1, 1, 1, 1)
+    n = _lib.load().ks_match_batches_workspace_size(C.byref(rd), len(recs), C.byref(bd),
+                                                    len(items), _PROJECTIONS[projection],
+                                                    int(teams))
+    if n == 0:
+        raise _lib.KilosortB200Error(_lib.KS_ERR_ARG, "ks_match_batches_workspace_size: "
+                                     + _lib.load().ks_last_error().decode(errors="replace"))
+    return n
+
+
+def _launch(recs, items, outs, info, ws, projection, teams):
+    rd, bd = _descs(recs, items, outs, info)
+    lib = _lib.load()
+    _lib.check(lib.ks_match_batches(C.byref(rd), len(recs), C.byref(bd), len(items),
+                                    _PROJECTIONS[projection], int(teams), _ptr(ws), ws.numel(),
+                                    _stream(ws.device)), "ks_match_batches")
+
+
+def _results(outs, info, what="ks_match_batches"):
+    """(st, amps, th_amps, Xres) per batch; raises on the first failed batch."""
+    host = info.cpu().tolist()
+    res = []
+    for i, (o, (n, status, _it, need)) in enumerate(zip(outs, host)):
+        if status == _lib.KS_ERR_OVERFLOW:
+            raise RuntimeError(f"{what}: batch {i} needs {need} spikes, above the capacity "
+                               f"{o.st.shape[0]} of its recording")
+        if status != _lib.KS_OK:
+            raise _lib.KilosortB200Error(status, f"{what}: batch {i}: device status {status}")
+        res.append((o.st[:n], o.amps[:n], o.th_amps[:n], o.Xres))
+    return res
+
+
+def match_batches(recs: Sequence[Recording], items: Sequence[Tuple[torch.Tensor, int]],
+                  projection: str = "bf16x3", teams: int = 0):
+    """Match every ``(X, recording index)`` of ``items``.
+
+    Returns a list of ``(st, amps, th_amps, Xres)``, one per batch, equal to
+    what ``run_matching`` returns for that batch alone.  Groups larger than
+    256 batches are split into consecutive calls.
+    """
+    recs = list(recs)
+    items = [(_need(X, "X", ndim=2), int(r)) for X, r in items]
+    out = []
+    for g0 in range(0, len(items), _lib.KS_MAX_BATCHES):
+        grp = items[g0:g0 + _lib.KS_MAX_BATCHES]
+        dev = _check_group(recs, grp)
+        outs = [_Outputs(recs[r], X.shape[0], X.shape[1], dev) for X, r in grp]
+        info = torch.empty((len(grp), 4), dtype=torch.int64, device=dev)
+        ws = torch.empty(workspace_size(recs, grp, projection, teams), dtype=torch.uint8,
+                         device=dev)
+        _launch(recs, grp, outs, info, ws, projection, teams)
+        out.extend(_results(outs, info))
+    return out
+
+
+# ------------------------------------------------------------------ autotuner
+_TEAMS_CACHE: Dict[tuple, int] = {}
+
+
+def _signature(recs, lengths_recs, projection):
+    dev = recs[0].U.device
+    return (torch.cuda.get_device_name(dev), projection,
+            tuple((r.shape, r.nt, int(r.max_peels)) for r in recs),
+            tuple(sorted(lengths_recs)))
+
+
+def autotune_teams(recs: Sequence[Recording], items: Sequence[Tuple[torch.Tensor, int]],
+                   projection: str = "bf16x3", candidates=(1, 2, 4, 8, 16, 32),
+                   reps: int = 2) -> int:
+    """Fastest team count for this workload, timed with CUDA events.
+
+    Every candidate runs the full call (warm-up once, then ``reps`` timed
+    runs); the winner is cached per (device, projection, template-set shapes,
+    batch lengths) so later calls with the same signature skip the search.
+    """
+    recs = list(recs)
+    items = [(_need(X, "X", ndim=2), int(r)) for X, r in items]
+    key = _signature(recs, [(X.shape[1], r) for X, r in items], projection)
+    if key in _TEAMS_CACHE:
+        return _TEAMS_CACHE[key]
+    dev = _check_group(recs, items)
+    outs = [_Outputs(recs[r], X.shape[0], X.shape[1], dev) for X, r in items]
+    info = torch.empty((len(items), 4), dtype=torch.int64, device=dev)
+    cands = [t for t in candidates if 1 <= t <= len(items)] or [1]
+    ws = torch.empty(max(workspace_size(recs, items, projection, t) for t in cands),
+                     dtype=torch.uint8, device=dev)
+    best, best_ms = cands[0], float("inf")
+    for t in cands:
+        _launch(recs, items, outs, info, ws, projection, t)
+        _results(outs, info, "autotune_teams")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            _launch(recs, items, outs, info, ws, projection, t)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        _results(outs, info, "autotune_teams")
+        ms = e0.elapsed_time(e1) / reps
+        if ms < best_ms:
+            best, best_ms = t, ms
+    _TEAMS_CACHE[key] = best
+    return best
+
+
+# ------------------------------------------------------------------ fixed shapes
+class BatchedMatcher:
+    """Repeated matching of batches with fixed shapes, optionally as a CUDA graph.
+
+    ``lengths`` lists ``(L, recording index)`` per batch.  The matcher owns
+    input buffers ``X[i]`` (fill them, e.g. ``X[i].copy_(pinned, non_blocking=True)``),
+    outputs and workspace, so the launch sequence can be captured once
+    (``graph=True``) and replayed with no per-call host work beyond the replay.
+    ``teams=None`` runs the autotuner on the first inputs given to ``run``.
+    """
+
+    def __init__(self, recs: Sequence[Recording], lengths: Sequence[Tuple[int, int]],
+                 projection: str = "bf16x3", teams: Optional[int] = 0, graph: bool = True,
+                 in_place: bool = False, workspace: Optional[torch.Tensor] = None):
+        if projection not in _PROJECTIONS:
+            raise ValueError(f"projection must be one of {sorted(_PROJECTIONS)}")
+        if len(lengths) > _lib.KS_MAX_BATCHES:
+            raise ValueError(f"at most {_lib.KS_MAX_BATCHES} batches")
+        self.recs = list(recs)
+        self.projection = projection
+        self.graph_enabled = graph
+        dev = self.recs[0].U.device
+        self.device = dev
+        self.X = [torch.zeros((self.recs[r].shape[0], int(L)), dtype=torch.float32, device=dev)
+                  for L, r in lengths]
+        self.items = [(X, int(r)) for X, (_, r) in zip(self.X, lengths)]
+        _check_group(self.recs, self.items)
+        self.outs = [_Outputs(self.recs[r], X.shape[0], X.shape[1], dev,
+                              Xres=X if in_place else None) for X, r in self.items]
+        self.info = torch.empty((len(self.items), 4), dtype=torch.int64, device=dev)
+        self.teams = teams
+        # matchers whose launches never overlap (one stream) may share one
+        # workspace of the largest size they need (workspace_bytes())
+        self._ws = workspace
+        self._graph = None
+
+    def workspace_bytes(self, teams: Optional[int] = None) -> int:
+        t = self.teams if teams is None else teams
+        return workspace_size(self.recs, self.items, self.projection, 0 if t is None else t)
+
+    def _prepare(self):
+        if self.teams is None:
+            self.teams = autotune_teams(self.recs, self.items, self.projection)
+        need = workspace_size(self.recs, self.items, self.projection, self.teams)
+        if self._ws is None:
+            self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+        elif self._ws.numel() < need or self._ws.device != self.device:
+            raise ValueError(f"shared workspace holds {self._ws.numel()} bytes, need {need}")
+
+    def launch(self):
+        """Enqueue one matching pass on the current stream (no host sync)."""
+        self._prepare()
+        if self.graph_enabled:
+            if self._graph is None:
+                _launch(self.recs, self.items, self.outs, self.info, self._ws, self.projection,
+                        self.teams)                # warm-up: first-use set-up out of capture
+                torch.cuda.synchronize(self.device)
+                g = torch.cuda.CUDAGraph()
+                s = torch.cuda.Stream(self.device)
+                s.wait_stream(torch.cuda.current_stream(self.device))
+                with torch.cuda.stream(s):
+                    g.capture_begin(capture_error_mode="thread_local")
+                    try:
+                        _launch(self.recs, self.items, self.outs, self.info, self._ws,
+                                self.projection, self.teams)
+                    finally:
+                        g.capture_end()
+                torch.cuda.current_stream(self.device).wait_stream(s)
+                self._graph = g
+            self._graph.replay()
+        else:
+            _launch(self.recs, self.items, self.outs, self.info, self._ws, self.projection,
+                    self.teams)
+
+    def results(self):
+        """Per batch ``(st, amps, th_amps, Xres)`` (synchronises to read the status).
+
+        The tensors are views of the matcher's own buffers: the next launch
+        overwrites them (clone what must outlive it).
+        """
+        return _results(self.outs, self.info)
+
+    def run(self, Xs: Optional[Sequence[torch.Tensor]] = None):
+        if Xs is not None:
+            if len(Xs) != len(self.X):
+                raise ValueError(f"expected {len(self.X)} batches")
+            for dst, src in zip(self.X, Xs):
+                dst.copy_(src, non_blocking=True)
+        self.launch()
+        return self.results()

@@ -43,7 +43,20 @@ int device_info(DeviceInfo* out) {
   return KS_OK;
 }
 
-static unsigned long long wait_limit_ns() {
+// Per host thread: events recorded at the stage boundaries of the calls it
+// makes while tracing is on.
+struct TraceState {
+  bool on = false;
+  int device = -1;
+  cudaEvent_t ev[kTraceMarks] = {};
+};
+static thread_local TraceState g_trace;
+
+void trace_mark(int slot, cudaStream_t stream) {
+  if (g_trace.on && slot >= 0 && slot < kTraceMarks) cudaEventRecord(g_trace.ev[slot], stream);
+}
+
+unsigned long long wait_limit_ns() {
   static unsigned long long v = [] {
     const char* s = std::getenv("KS_B200_WAIT_LIMIT_NS");
     unsigned long long x = s ? std::strtoull(s, nullptr, 10) : 0ull;
@@ -247,10 +260,12 @@ int ks_run_matching(const float* X, const float* U, const float* W, const float*
     if (rc) return rc;
     ctcT = t;
   }
+  trace_mark(0, s);
   if (Xres != X)
     KS_CUDA(cudaMemcpyAsync(Xres, X, sizeof(float) * C * L, cudaMemcpyDeviceToDevice, s));
   rc = launch_template_energy(U, K, P, C, nm, s);
   if (rc) return rc;
+  trace_mark(1, s);
   rc = launch_project(X, U, W, C, L, K, P, nt, precision, Bt, 0, true, base + m.proj_off,
                       m.ctc_off - m.proj_off, nullptr, s);
   if (rc) return rc;
@@ -289,6 +304,32 @@ int ks_ctc(const float* U, const float* W, int64_t K, int64_t P, int64_t C,
            void* stream) {
   return launch_ctc(U, W, K, P, C, nt, ctc, workspace, workspace_bytes,
                     static_cast<cudaStream_t>(stream));
+}
+
+int ks_trace_stages(int enable) {
+  if (!enable) {
+    g_trace.on = false;
+    return KS_OK;
+  }
+  DeviceInfo d;
+  int rc = device_info(&d);
+  if (rc) return rc;
+  if (g_trace.device != d.device) {
+    for (int i = 0; i < kTraceMarks; ++i)
+      if (g_trace.ev[i]) cudaEventDestroy(g_trace.ev[i]);
+    for (int i = 0; i < kTraceMarks; ++i) KS_CUDA(cudaEventCreate(&g_trace.ev[i]));
+    g_trace.device = d.device;
+  }
+  g_trace.on = true;
+  return KS_OK;
+}
+
+int ks_trace_read(float* ms, int n) {
+  if (!ms || n < 1 || n > kTraceMarks - 1) return fail(KS_ERR_ARG, "ks_trace_read: 1..4 intervals");
+  if (g_trace.device < 0) return fail(KS_ERR_ARG, "ks_trace_read: tracing was never enabled");
+  KS_CUDA(cudaEventSynchronize(g_trace.ev[n]));
+  for (int i = 0; i < n; ++i) KS_CUDA(cudaEventElapsedTime(&ms[i], g_trace.ev[i], g_trace.ev[i + 1]));
+  return KS_OK;
 }
 
 int ks_selftest_wait(int64_t timeout_ns, int* status, void* stream) {

@@ -19,11 +19,16 @@
 //              are one contiguous 4 KB run)
 // Tiles are (128 templates) x (256 samples), template tiles of one sample tile
 // consecutive so concurrent CTAs share the Y tile through L2.  No TMA multicast.
+// One launch can cover many batches of up to kGroupRecs recordings: the tile
+// table (GemmGroup, a __grid_constant__ parameter with the tensor maps of each
+// recording) maps a global tile number to (batch, template tile, sample tile);
+// the Y operands of a recording's batches are stacked in one tensor and each
+// batch reads its own row range.
 // Every mbarrier wait is bounded by %globaltimer; a wait that runs out sets the
 // error word, the CTA drains its own copies in flight (bounded), frees TMEM and
 // returns.
 #include "ks_common.cuh"
-#include "project.cuh"
+#include "gemm_group.cuh"
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -141,19 +146,21 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-struct GemmArgs {
-  float* B;
-  long long ldb;
-  int tiled;
-  int K, L, nk, tiles_m, n_tiles;
-  int* err;
-};
+using ks::GemmBatch;
+using ks::GemmGroup;
+
+// Batch of global tile t (the batches' tile ranges are consecutive).
+__device__ __forceinline__ int tile_batch(const GemmGroup& g, int t) {
+  int lo = 0, hi = g.n_batches - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (g.batches[mid].tile_begin <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
 
 __global__ void __launch_bounds__(kThreads, 1)
-ks_bf16x3_kernel(const __grid_constant__ CUtensorMap map_uhi,
-                 const __grid_constant__ CUtensorMap map_ulo,
-                 const __grid_constant__ CUtensorMap map_yhi,
-                 const __grid_constant__ CUtensorMap map_ylo, GemmArgs g) {
+ks_bf16x3_kernel(const __grid_constant__ GemmGroup g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // 1024-byte alignment for the swizzled tiles
   const uint32_t raw = smem_u32(smem_raw);
@@ -202,17 +209,21 @@ ks_bf16x3_kernel(const __grid_constant__ CUtensorMap map_uhi,
       uint32_t pend_ph[kStages] = {}; // ... completing this phase of full[stage]
       bool ok = true;
       for (int t = blockIdx.x; ok && t < g.n_tiles; t += gridDim.x) {
-        const int m0 = (t % g.tiles_m) * kBM;
-        const int n0 = (t / g.tiles_m) * kBN;
-        for (int kb = 0; kb < g.nk; ++kb) {
+        const GemmBatch& bt = g.batches[tile_batch(g, t)];
+        const int lt = t - bt.tile_begin;
+        const int m0 = (lt % bt.tiles_m) * kBM;
+        const int y0 = bt.row_off + (lt / bt.tiles_m) * kBN;
+        const CUtensorMap* maps = g.maps[bt.rec];
+        const int nk = g.nk[bt.rec];
+        for (int kb = 0; kb < nk; ++kb) {
           if (!mbar_wait(empty0 + 8 * s, ph ^ 1u, g.err)) { ok = false; break; }
           const uint32_t st = base + s * kStageBytes;
           const uint32_t fb = full0 + 8 * s;
           mbar_expect_tx(fb, kStageBytes);
-          tma_load_2d(st, &map_uhi, kb * kBK, m0, fb);
-          tma_load_2d(st + kTileA, &map_ulo, kb * kBK, m0, fb);
-          tma_load_2d(st + 2 * kTileA, &map_yhi, kb * kBK, n0, fb);
-          tma_load_2d(st + 2 * kTileA + kTileB, &map_ylo, kb * kBK, n0, fb);
+          tma_load_2d(st, &maps[0], kb * kBK, m0, fb);
+          tma_load_2d(st + kTileA, &maps[1], kb * kBK, m0, fb);
+          tma_load_2d(st + 2 * kTileA, &maps[2], kb * kBK, y0, fb);
+          tma_load_2d(st + 2 * kTileA + kTileB, &maps[3], kb * kBK, y0, fb);
           pending[s] = true;
           pend_ph[s] = ph;
           if (++s == kStages) { s = 0; ph ^= 1u; }
@@ -241,7 +252,8 @@ ks_bf16x3_kernel(const __grid_constant__ CUtensorMap map_uhi,
         if (!mbar_wait(tempty0 + 8 * acc, acc_ph ^ 1u, g.err)) { ok = false; break; }
         fence_after();
         const uint32_t d = tmem + (uint32_t)(acc * kBN);
-        for (int kb = 0; kb < g.nk; ++kb) {
+        const int nk = g.nk[g.batches[tile_batch(g, t)].rec];
+        for (int kb = 0; kb < nk; ++kb) {
           if (!mbar_wait(full0 + 8 * s, ph, g.err)) { ok = false; break; }
           fence_after();
           const uint32_t st = base + s * kStageBytes;
@@ -277,9 +289,12 @@ ks_bf16x3_kernel(const __grid_constant__ CUtensorMap map_uhi,
     int acc = 0;
     uint32_t acc_ph = 0;
     for (int t = blockIdx.x; t < g.n_tiles; t += gridDim.x) {
-      const int m0 = (t % g.tiles_m) * kBM;
-      const int n0 = (t / g.tiles_m) * kBN;
-      if (!mbar_wait(tfull0 + 8 * acc, acc_ph, g.err)) break;
+      const GemmBatch& bt = g.batches[tile_batch(g, t)];
+      const int lt = t - bt.tile_begin;
+      const int m0 = (lt % bt.tiles_m) * kBM;
+      const int n0 = (lt / bt.tiles_m) * kBN;
+      // the warp leaves together (tcgen05.ld below needs every lane)
+      if (!__all_sync(0xffffffffu, mbar_wait(tfull0 + 8 * acc, acc_ph, g.err))) break;
       fence_after();
       const int row = m0 + q * 32 + lane;    // template of this thread
       const uint32_t tl = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * kBN);
@@ -288,11 +303,17 @@ ks_bf16x3_kernel(const __grid_constant__ CUtensorMap map_uhi,
         uint32_t r[32];
         tmem_ld32(tl + (uint32_t)(c * 32), r);
         const int n = n0 + c * 32;
-        if (row < g.K && n < g.L) {
-          float* dst = g.tiled ? g.B + ((size_t)(n >> 5) * g.K + row) * 32
-                               : g.B + (size_t)row * g.ldb + n;
-          const bool full = n + 32 <= g.L && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
+        if (row < bt.K && n < bt.L) {
+          float* dst = g.tiled ? bt.B + ((size_t)(n >> 5) * bt.K + row) * 32
+                               : bt.B + (size_t)row * bt.ldb + n;
+          // the tiled layout's last block is written whole (zeros past L)
+          const bool full = (g.tiled || n + 32 <= bt.L) &&
+                            ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
           if (full) {
+            const int nv = bt.L - n;   // valid columns of this block (>= 1)
+#pragma unroll
+            for (int e = 0; e < 32; ++e)
+              if (e >= nv) r[e] = 0u;
 #pragma unroll
             for (int v = 0; v < 8; ++v)
               reinterpret_cast<float4*>(dst)[v] =
@@ -301,7 +322,7 @@ ks_bf16x3_kernel(const __grid_constant__ CUtensorMap map_uhi,
           } else {
 #pragma unroll
             for (int e = 0; e < 32; ++e)
-              if (n + e < g.L) dst[e] = __uint_as_float(r[e]);
+              if (n + e < bt.L) dst[e] = __uint_as_float(r[e]);
           }
         }
       }
@@ -361,6 +382,35 @@ int make_map(CUtensorMap* map, const __nv_bfloat16* ptr, int64_t rows, int64_t c
 
 namespace ks {
 
+int make_bf16_map(CUtensorMap* map, const __nv_bfloat16* ptr, int64_t rows, int64_t cols,
+                  int box_rows) {
+  if (reinterpret_cast<uintptr_t>(ptr) & 15) return fail(KS_ERR_ARG, "bf16x3: operands must be 16-byte aligned");
+  return make_map(map, ptr, rows, cols, box_rows);
+}
+
+int gemm_tile_n() { return kBN; }
+int gemm_tile_m() { return kBM; }
+
+int launch_gemm_group(GemmGroup& g, cudaStream_t stream) {
+  if (g.n_batches < 1 || g.n_batches > kGroupBatches) return fail(KS_ERR_ARG, "bf16x3: bad group size");
+  if (!g.err) return fail(KS_ERR_ARG, "bf16x3: error word missing");
+  DeviceInfo dev;
+  int rc = device_info(&dev);
+  if (rc) return rc;
+  const size_t smem = (size_t)kStages * kStageBytes + 1024 + 256;
+  static thread_local int attr_device = -1;
+  if (attr_device != dev.device) {
+    KS_CUDA(cudaFuncSetAttribute(ks_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    attr_device = dev.device;
+  }
+  const int grid = std::min(dev.sm_count, g.n_tiles);
+  if (grid < 1) return KS_OK;
+  ks_bf16x3_kernel<<<grid, kThreads, smem, stream>>>(g);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
 int gemm_bf16x3(const __nv_bfloat16* Uhi, const __nv_bfloat16* Ulo, const __nv_bfloat16* Yhi,
                 const __nv_bfloat16* Ylo, float* B, int64_t K, int64_t L, int64_t Q,
                 int64_t Kpad, int64_t Lpad, int64_t ldb, bool tiled, int* err,
@@ -368,38 +418,27 @@ int gemm_bf16x3(const __nv_bfloat16* Uhi, const __nv_bfloat16* Ulo, const __nv_b
   if (!err) return fail(KS_ERR_ARG, "bf16x3: error word missing");
   if (Q % kBK) return fail(KS_ERR_ARG, "bf16x3: contraction length must be a multiple of 64");
   if (Kpad % kBM) return fail(KS_ERR_ARG, "bf16x3: template rows must be padded to 128");
-  const uintptr_t al = reinterpret_cast<uintptr_t>(Uhi) | reinterpret_cast<uintptr_t>(Ulo) |
-                       reinterpret_cast<uintptr_t>(Yhi) | reinterpret_cast<uintptr_t>(Ylo);
-  if (al & 15) return fail(KS_ERR_ARG, "bf16x3: operands must be 16-byte aligned");
-  DeviceInfo dev;
-  int rc = device_info(&dev);
-  if (rc) return rc;
-  CUtensorMap m_uhi, m_ulo, m_yhi, m_ylo;
-  if ((rc = make_map(&m_uhi, Uhi, Kpad, Q, kBM))) return rc;
-  if ((rc = make_map(&m_ulo, Ulo, Kpad, Q, kBM))) return rc;
-  if ((rc = make_map(&m_yhi, Yhi, Lpad, Q, kBN))) return rc;
-  if ((rc = make_map(&m_ylo, Ylo, Lpad, Q, kBN))) return rc;
-  GemmArgs g;
-  g.B = B;
-  g.ldb = ldb;
+  static thread_local GemmGroup g;   // about 14 KB: kept off the stack
+  int rc;
+  if ((rc = make_bf16_map(&g.maps[0][0], Uhi, Kpad, Q, kBM))) return rc;
+  if ((rc = make_bf16_map(&g.maps[0][1], Ulo, Kpad, Q, kBM))) return rc;
+  if ((rc = make_bf16_map(&g.maps[0][2], Yhi, Lpad, Q, kBN))) return rc;
+  if ((rc = make_bf16_map(&g.maps[0][3], Ylo, Lpad, Q, kBN))) return rc;
+  g.nk[0] = (int)(Q / kBK);
+  GemmBatch& b = g.batches[0];
+  b.B = B;
+  b.ldb = ldb;
+  b.K = (int)K;
+  b.L = (int)L;
+  b.rec = 0;
+  b.row_off = 0;
+  b.tiles_m = (int)(Kpad / kBM);
+  b.tile_begin = 0;
+  g.n_batches = 1;
+  g.n_tiles = b.tiles_m * (int)((L + kBN - 1) / kBN);
   g.tiled = tiled ? 1 : 0;
-  g.K = (int)K;
-  g.L = (int)L;
-  g.nk = (int)(Q / kBK);
-  g.tiles_m = (int)(Kpad / kBM);
-  g.n_tiles = g.tiles_m * (int)((L + kBN - 1) / kBN);
   g.err = err;
-  const size_t smem = (size_t)kStages * kStageBytes + 1024 + 256;
-  static int attr_device = -1;
-  if (attr_device != dev.device) {
-    KS_CUDA(cudaFuncSetAttribute(ks_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-    attr_device = dev.device;
-  }
-  const int grid = std::min(dev.sm_count, g.n_tiles);
-  ks_bf16x3_kernel<<<grid, kThreads, smem, stream>>>(m_uhi, m_ulo, m_yhi, m_ylo, g);
-  KS_CUDA(cudaGetLastError());
-  return KS_OK;
+  return launch_gemm_group(g, stream);
 }
 
 }  // namespace ks

@@ -48,6 +48,12 @@ struct Carve {
 
 // Default limit of every device-side wait (ns of %globaltimer).
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+// kWaitLimitNs, or KS_B200_WAIT_LIMIT_NS from the environment when set.
+unsigned long long wait_limit_ns();
+// Stage marks of ks_trace_stages: record the calling thread's event `slot`
+// on the stream when tracing is on (no-op otherwise).
+constexpr int kTraceMarks = 5;
+void trace_mark(int slot, cudaStream_t stream);
 
 }  // namespace ks
 
@@ -75,12 +81,16 @@ __device__ __forceinline__ int ks_ld_volatile(const int* p) {
 // to order.  Every block passes the same sequence of barriers and keeps its own
 // epoch.  A wait that exceeds limit_ns records KS_ERR_TIMEOUT in *err and
 // returns; every caller then sees the error flag and leaves its loop, so no
-// block waits without bound.  Returns true when no error is recorded.
+// block waits without bound.  Returns true when no error is recorded; the
+// answer is the same for every thread of the block (thread 0 reads the flag
+// and the closing barrier broadcasts it), so callers may branch on it around
+// further block barriers.
 __device__ __forceinline__ bool ks_grid_sync(unsigned* count, unsigned nblocks,
                                              unsigned& epoch, int* err,
                                              unsigned long long limit_ns) {
   __syncthreads();
   ++epoch;
+  int bad = 0;
   if (threadIdx.x == 0) {
     const unsigned target = epoch * nblocks;
     __threadfence();
@@ -96,7 +106,7 @@ __device__ __forceinline__ bool ks_grid_sync(unsigned* count, unsigned nblocks,
       }
     }
     __threadfence();
+    bad = ks_ld_volatile(err) != 0;
   }
-  __syncthreads();
-  return ks_ld_volatile(err) == 0;
+  return __syncthreads_or(bad) == 0;
 }

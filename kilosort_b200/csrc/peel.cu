@@ -129,12 +129,15 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
   cfg.stream = stream;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  trace_mark(2, stream);
   KS_CUDA(cudaLaunchKernelEx(&cfg, peel_kernel, a));
+  trace_mark(3, stream);
   // residual updates of all recorded spikes
   const long long n_res = (long long)a.nblk * ((C + 31) / 32);
   const unsigned rgrid = (unsigned)((n_res + kResWarps - 1) / kResWarps);
   ks_residual_kernel<<<rgrid, kResThreads, residual_smem_bytes(a.P, a.nt), stream>>>(a);
   KS_CUDA(cudaGetLastError());
+  trace_mark(4, stream);
   return KS_OK;
 }
 

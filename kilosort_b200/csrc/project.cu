@@ -219,6 +219,8 @@ ks_sgemm_tn_kernel(const float* __restrict__ A, const float* __restrict__ Bt,
     if (kt + 1 < nk) sstore(buf ^ 1);
     __syncthreads();
   }
+  // the tiled layout's last block is written whole: columns past N get zeros
+  const long long nw = kTiled ? (((long long)N + 31) & ~31LL) : N;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const long long m = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
@@ -227,12 +229,14 @@ ks_sgemm_tn_kernel(const float* __restrict__ A, const float* __restrict__ Bt,
     for (int h = 0; h < 2; ++h) {
       const long long n = n0 + h * 64 + tx * 4;
       float* dst = kTiled ? Cm + (((n >> 5) * M + m) << 5) + (n & 31) : Cm + m * ldc + n;
-      const float* v = &acc[i][h * 4];
-      if (n + 3 < N && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0)) {
+      float v[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) v[e] = n + e < N ? acc[i][h * 4 + e] : 0.f;
+      if (n + 3 < nw && ((reinterpret_cast<uintptr_t>(dst) & 15) == 0)) {
         *reinterpret_cast<float4*>(dst) = make_float4(v[0], v[1], v[2], v[3]);
       } else {
         for (int e = 0; e < 4; ++e)
-          if (n + e < N) dst[e] = v[e];
+          if (n + e < nw) dst[e] = v[e];
       }
     }
   }
@@ -280,6 +284,16 @@ int launch_template_energy(const float* U, int64_t K, int64_t P, int64_t C,
   const int threads = 256;
   const long long blocks = (K * 32 + threads - 1) / threads;
   ks_template_energy_kernel<<<(unsigned)blocks, threads, 0, stream>>>(U, (int)K, (int)P, (int)C, nm);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
+int launch_reorder_templates(const float* U, int64_t K, int64_t P, int64_t C, int64_t Kpad,
+                             int64_t Q, float* Uf, __nv_bfloat16* Uhi, __nv_bfloat16* Ulo,
+                             cudaStream_t stream) {
+  const int blocks = (int)std::min<int64_t>(4096, (Kpad * Q + 255) / 256);
+  ks_reorder_templates_kernel<<<blocks, 256, 0, stream>>>(U, (int)K, (int)P, (int)C, (int)Kpad,
+                                                          (int)Q, Uf, Uhi, Ulo);
   KS_CUDA(cudaGetLastError());
   return KS_OK;
 }

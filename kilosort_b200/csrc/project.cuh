@@ -1,10 +1,23 @@
 // Internal interfaces of the projection kernels.
 #pragma once
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace ks {
+
+constexpr int kGroupRecs = 8;       // recordings in one grouped contraction
+constexpr int kGroupBatches = 256;  // batches in one grouped contraction
+struct GemmGroup;
+// Grouped split-BF16 contraction over the tiles of several batches/recordings
+// (gemm_bf16x3.cu); the caller fills maps, nk, batches, n_batches, n_tiles, tiled, err.
+int launch_gemm_group(GemmGroup& g, cudaStream_t stream);
+// Tensor map of a bf16 [rows][cols] operand, boxes of box_rows x 64.
+int make_bf16_map(CUtensorMap* map, const __nv_bfloat16* ptr, int64_t rows, int64_t cols,
+                  int box_rows);
+int gemm_tile_n();
+int gemm_tile_m();
 
 struct ProjLayout {
   int64_t Q;      // contraction length, q = c*P + p, padded to 64
@@ -16,6 +29,14 @@ ProjLayout proj_layout(int64_t C, int64_t L, int64_t K, int64_t P, int precision
 
 int launch_template_energy(const float* U, int64_t K, int64_t P, int64_t C,
                            float* nm, cudaStream_t stream);
+// U [K,P,C] -> [Kpad][Q] (q = c*P + p, zero padded): f32 (Uf) and/or bf16 hi/lo.
+int launch_reorder_templates(const float* U, int64_t K, int64_t P, int64_t C, int64_t Kpad,
+                             int64_t Q, float* Uf, __nv_bfloat16* Uhi, __nv_bfloat16* Ulo,
+                             cudaStream_t stream);
+// X [C,L] -> Y [Lpad][Q] rows (f32 and/or bf16 hi/lo); Y is written for rows < Lpad.
+int launch_temporal(const float* X, const float* W, int64_t C, int64_t L, int64_t P,
+                    int64_t nt, int64_t Q, int64_t Lpad, float* Yf, __nv_bfloat16* Yhi,
+                    __nv_bfloat16* Ylo, cudaStream_t stream);
 // B is written row-major [K, ldb] or, when tiled, in 32-column blocks
 // [ceil(L/32)][K][32] (the layout of the peel).
 // The first 256 bytes of the workspace hold the device error word of the
@@ -43,6 +64,9 @@ int launch_untile_rows(const float* Bt, int64_t K, int64_t L, float* B, int64_t 
                        cudaStream_t stream);
 int launch_ctc_transpose(const float* ctc, int64_t K, int64_t nt, float* ctcT,
                          cudaStream_t stream);
+int check_peel_shape(int64_t C, int64_t L, int64_t K, int64_t P, int64_t nt, float th2,
+                     int64_t max_peels, int64_t capacity);
+int launch_nm_pairs(const float* nm, int64_t K, float2* nmi, cudaStream_t stream);
 int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
                       const float* ctcT, const float* nm, int64_t C, int64_t L, int64_t K,
                       int64_t P, int64_t nt, float th2, int64_t max_peels,

@@ -266,11 +266,12 @@ def run_matching(ops, X, U, ctc, device=torch.device("cuda")):
         else DEFAULT_CAPACITY
     prec = _projection(ops)
     dev = X.device
-    st = torch.zeros((capacity, 2), dtype=torch.int64, device=dev)
-    amps = torch.zeros((capacity, 1), dtype=torch.float32, device=dev)
-    th_amps = torch.zeros((capacity, 1), dtype=torch.float32, device=dev)
+    # only the first info[0] rows are returned, and the peel writes all of info
+    st = torch.empty((capacity, 2), dtype=torch.int64, device=dev)
+    amps = torch.empty((capacity, 1), dtype=torch.float32, device=dev)
+    th_amps = torch.empty((capacity, 1), dtype=torch.float32, device=dev)
     Xres = torch.empty_like(X)
-    info = torch.zeros(4, dtype=torch.int64, device=dev)
+    info = torch.empty(4, dtype=torch.int64, device=dev)
     lib = _lib.load()
     ctcT = _ctcT.get(ctc, nt)
     ws = _ws.get(dev, lib.ks_run_matching_workspace_size(Cn, L, K, P, nt, prec,

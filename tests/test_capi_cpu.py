@@ -61,3 +61,62 @@ def test_python_layer_refuses_cpu_tensors():
     with pytest.raises(ValueError, match="CUDA"):
         kb.run_matching(ops, torch.zeros(4, 200), torch.zeros(2, 6, 4),
                         torch.zeros(2, 2, 123))
+
+
+def test_descriptor_structs_match_the_c_layout(tmp_path):
+    """ks_rec_desc / ks_batch_desc: ctypes mirrors agree with the C compiler."""
+    import os
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "ks_b200.h"\n'
+        "int main(void) {\n"
+        '  printf("%zu %zu %zu %zu %zu\\n", sizeof(ks_rec_desc), offsetof(ks_rec_desc, th2),\n'
+        "         offsetof(ks_rec_desc, max_peels), offsetof(ks_rec_desc, capacity),\n"
+        "         offsetof(ks_rec_desc, nt));\n"
+        '  printf("%zu %zu %zu %zu\\n", sizeof(ks_batch_desc), offsetof(ks_batch_desc, L),\n'
+        "         offsetof(ks_batch_desc, rec), offsetof(ks_batch_desc, info));\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(_lib.HEADER))
+    subprocess.run([cc, "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    r = [int(v) for v in out[0].split()]
+    b = [int(v) for v in out[1].split()]
+    R, B = _lib.RecDesc, _lib.BatchDesc
+    assert r == [ctypes.sizeof(R), R.th2.offset, R.max_peels.offset, R.capacity.offset,
+                 R.nt.offset]
+    assert b == [ctypes.sizeof(B), B.L.offset, B.rec.offset, B.info.offset]
+
+
+def test_batched_workspace_query_and_argument_checks():
+    lib = _lib.load()
+    recs = (_lib.RecDesc * 2)(
+        _lib.RecDesc(1, 1, 1, 384, 600, 6, 61, 64.0, 100, 100000),
+        _lib.RecDesc(1, 1, 1, 96, 150, 6, 61, 64.0, 100, 100000))
+    bats = (_lib.BatchDesc * 3)(
+        _lib.BatchDesc(1, 1, 60122, 0, 1, 1, 1, 1),
+        _lib.BatchDesc(1, 1, 20122, 1, 1, 1, 1, 1),
+        _lib.BatchDesc(1, 1, 8122, 0, 1, 1, 1, 1))
+    n_split = lib.ks_match_batches_workspace_size(recs, 2, bats, 3, _lib.KS_PROJ_BF16X3, 2)
+    n_fp32 = lib.ks_match_batches_workspace_size(recs, 2, bats, 3, _lib.KS_PROJ_FP32, 2)
+    # tiled scores of every batch at least
+    assert n_split > 4 * (600 * 60122 + 150 * 20122 + 600 * 8122)
+    assert n_fp32 > 4 * (600 * 60122 + 150 * 20122 + 600 * 8122)
+    # split form stacks the bf16 hi/lo projections of every batch of a recording
+    assert n_split > 2 * 2 * (60160 + 8192) * 2304
+    # more teams, more team scratch
+    assert lib.ks_match_batches_workspace_size(recs, 2, bats, 3, _lib.KS_PROJ_BF16X3, 3) > n_split
+    # a bad recording index, too many batches and a bad precision are refused
+    bats[1].rec = 5
+    assert lib.ks_match_batches_workspace_size(recs, 2, bats, 3, _lib.KS_PROJ_BF16X3, 2) == 0
+    assert b"recording index" in lib.ks_last_error()
+    bats[1].rec = 1
+    assert lib.ks_match_batches_workspace_size(recs, 2, bats, 300, _lib.KS_PROJ_BF16X3, 2) == 0
+    assert lib.ks_match_batches_workspace_size(recs, 2, bats, 3, 7, 2) == 0
+    rc = lib.ks_match_batches(recs, 2, bats, 3, _lib.KS_PROJ_BF16X3, 2, None, 0, None)
+    assert rc == _lib.KS_ERR_WORKSPACE
