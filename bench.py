@@ -51,9 +51,11 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batches", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="np1", choices=["np1", "uneven"],
+    p.add_argument("--workload", default="np1", choices=["np1", "uneven", "adjoint"],
                    help="np1: C=384/K=600, 20 equal batches (default); uneven: three "
-                        "recordings, 200 batches of uneven length, batched launches")
+                        "recordings, 200 batches of uneven length, batched launches; "
+                        "adjoint: reconstruction loss + hand-written adjoint on one "
+                        "C=384/K=600 batch with the matcher's spikes")
     p.add_argument("--group", type=int, default=50,
                    help="uneven workload: batches per batched call (one graph each)")
     return p.parse_args()
@@ -259,6 +261,69 @@ def uneven_main(args, dev, rank, world):
     if rank == 0:
         print(json.dumps(line), flush=True)
 
+ADJOINT = ("fixed-assignment reconstruction loss ||X - R||^2 and its adjoint (dU, dwPCA, "
+           "damps): C=384, K=600, one 60000-sample batch (+2*61 pad), spikes of the FP32 "
+           "matcher (synthetic seed 1004, 2-37 Hz)")
+
+
+def adjoint_main(args, dev, rank, world):
+    """Forward (ks_recon_loss) and backward (ks_recon_adjoint) per step."""
+    import kilosort_b200 as kb
+    from kilosort_b200 import synth
+    from kilosort_b200.adjoint import reconstruction_loss
+    rec = synth.config_recording(4)
+    U = torch.from_numpy(rec.U).to(dev)
+    W = torch.from_numpy(rec.wPCA).to(dev)
+    X = torch.from_numpy(np.ascontiguousarray(rec.batch(0))).to(dev)
+    ops = dict(Th_learned=TH, nt=NT, max_peels=100, wPCA=W)
+    ctc = kb.prepare_matching(ops, U)
+    st, amps, _, _ = kb.run_matching(dict(ops, projection="fp32"), X, U, ctc, device=dev)
+    amps = amps.reshape(-1)
+    C, L = X.shape
+    K = U.shape[0]
+    N = len(st)
+    Uq, Wq, aq = (t.clone().requires_grad_(True) for t in (U, W, amps))
+
+    def step():
+        for t in (Uq, Wq, aq):
+            t.grad = None
+        reconstruction_loss(X, st, aq, Uq, Wq).backward()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev.index or 0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler.__enter__()
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    sampler.__exit__()
+    ms = e0.elapsed_time(e1) / args.steps
+    # window bytes the adjoint reads per spike (C x nt residual floats) and
+    # the flops of its per-spike work (H update, waveform dot product)
+    win_bytes = 4.0 * C * NT * N
+    samples = C * (L - 2 * NT)
+    line = {
+        "metric": "channel-samples/s", "value": samples * world / (ms * 1e-3),
+        "unit": "channel-samples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": ADJOINT, "spikes": N, "templates": K,
+                   "l2": "X, Xres 92 MB each: the residual windows are L2 reads",
+                   "parallelism": f"replicas x{world}"},
+        "spikes_per_s": N * world / (ms * 1e-3),
+        "window_gbs": win_bytes / (ms * 1e-3) / 1e9,
+        "clocks": sampler.summary(),
+        # forward: count, scan, fill, reconstruct, sum; backward: count, scan,
+        # group, adjoint, dW, damps
+        "gpu_launches": 11,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
 
 def main():
     args = parse()
@@ -276,8 +341,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
 
-    if args.workload == "uneven":
-        uneven_main(args, dev, rank, world)
+    if args.workload in ("uneven", "adjoint"):
+        (uneven_main if args.workload == "uneven" else adjoint_main)(args, dev, rank, world)
         if world > 1:
             dist.destroy_process_group()
         return

@@ -230,6 +230,36 @@ KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
                             size_t workspace_bytes, void* stream);
 
 /*
+ * Fixed-assignment reconstruction loss and its adjoint, for template
+ * refinement.  For spikes s = (tau_s = st[s][0], k_s = st[s][1]) with
+ * amplitudes amps[s]:
+ *   R[c, tau] = sum_s amps[s] * sum_p U[k_s,p,c] W[p, tau - tau_s + nt/2]
+ * (the subtraction of kilosort/template_matching.py:237 applied to a fixed
+ * spike set; window taps outside [0, L) are dropped), Xres = X - R and
+ * loss = sum (X - R)^2, written to *loss (device double).  ks_recon_adjoint
+ * takes that Xres and the upstream gradient dloss (device float) and writes
+ * dU [K,P,C], dW [P,nt] and damps [n_spikes] of dloss * loss; it recomputes
+ * the template waveforms U x W per block instead of storing them.  Both are
+ * deterministic (fixed summation orders).  A spike with tau outside [0, L) or
+ * a template outside [0, K) sets *status (device int) to KS_ERR_ARG and is
+ * skipped.  No counterpart in the reference (it has no gradient of the
+ * matching); the forward reproduces its residual subtraction.
+ */
+KS_API size_t ks_recon_workspace_size(int64_t C, int64_t L, int64_t K, int64_t P,
+                                      int64_t nt, int64_t n_spikes);
+KS_API int ks_recon_loss(const float* X, const int64_t* st, const float* amps,
+                         int64_t n_spikes, const float* U, const float* W, int64_t C,
+                         int64_t L, int64_t K, int64_t P, int64_t nt, float* Xres,
+                         double* loss, int* status, void* workspace,
+                         size_t workspace_bytes, void* stream);
+KS_API int ks_recon_adjoint(const float* Xres, const int64_t* st, const float* amps,
+                            int64_t n_spikes, const float* U, const float* W, int64_t C,
+                            int64_t L, int64_t K, int64_t P, int64_t nt,
+                            const float* dloss, float* dU, float* dW, float* damps,
+                            int* status, void* workspace, size_t workspace_bytes,
+                            void* stream);
+
+/*
  * Stage timing of ks_run_matching, for profiling the public call as it runs
  * (no work is skipped or added).  While enabled on the calling host thread,
  * ks_run_matching records CUDA events at five points on its stream: start,

@@ -60,6 +60,11 @@ SIGNATURES = {
     "ks_selftest_wait": (_int, [_i64, _vp, _vp]),
     "ks_peel_static": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
                               _f32, _i64, _i64, _vp, _vp, _vp, _vp, _vp]),
+    "ks_recon_workspace_size": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64]),
+    "ks_recon_loss": (_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
+                             _vp, _vp, _vp, _vp, _sz, _vp]),
+    "ks_recon_adjoint": (_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
+                                _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "ks_trace_stages": (_int, [_int]),
     "ks_trace_read": (_int, [_vp, _int]),
     "ks_match_batches_workspace_size": (_sz, [_vp, _i64, _vp, _i64, _int, _i64]),

@@ -245,7 +245,7 @@ CONFIGS = {
     2: dict(n_chan=384, probe="np1", n_templates=600, n_batches=20,
             rate_hz=(2.0, 15.0), amp_sd=(6.0, 30.0)),
     4: dict(n_chan=384, probe="np1", n_templates=600, n_batches=1,
-            rate_hz=(2.0, 15.0), amp_sd=(6.0, 30.0)),
+            rate_hz=(5.0, 37.0), amp_sd=(6.0, 30.0)),      # ~25000 spikes per batch
     5: dict(n_chan=384, probe="np1", n_templates=2000, n_batches=1800,
             rate_hz=(1.0, 30.0), amp_sd=(5.0, 40.0)),
 }
