@@ -345,6 +345,76 @@ def spike_features(Xres, st, amps, W, iCC, iU, Ucc):
     return tF
 
 
+def _match_features(ops, W, iCCd, iU, Ucc):
+    """Default per-batch matcher and feature step of `extract` (this library)."""
+    def match(X, U, ctc, device):
+        return run_matching(ops, X, U, ctc, device=device)
+
+    def features(Xres, st, amps):
+        return spike_features(Xres, st, amps, W, iCCd, iU, Ucc)     # [N, nC, P]
+    return match, features
+
+
+def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=None):
+    """Rows ``[N, 3]`` (time, template, th_amp; float64 numpy) and features
+    ``[N, nC, P]`` (CPU tensor) of the given batches, in batch order, before
+    the final sort -- the loop body of kilosort/template_matching.py:79-110.
+
+    ``match(X, U, ctc, device)`` returns ``(st, amps, th_amps, Xres)`` and
+    ``features(Xres, st, amps)`` the ``[N, nC, P]`` features of one batch.
+    """
+    try:
+        from tqdm import tqdm
+    except ImportError:  # pragma: no cover
+        tqdm = None
+    nt = ops["nt"]
+    nC = ops["settings"]["nearest_chans"]
+    st = np.zeros((10 ** 6, 3), "float64")
+    tF = torch.zeros((10 ** 6, nC, ops["settings"]["n_pcs"]))
+    k = 0
+    prog = tqdm(batches, miniters=200 if progress_bar else None,
+                mininterval=60 if progress_bar else None) if tqdm else batches
+    ibatch = -1
+    try:
+        for ibatch in prog:
+            ibatch = int(ibatch)
+            if ibatch % 100 == 0 and torch.cuda.is_available():
+                logger.debug(f"Batch {ibatch}: {torch.cuda.memory_allocated() / 2**30:.2f} GiB allocated")
+            X = bfile.padded_batch_to_torch(ibatch, ops)
+            stt, amps, th_amps, Xres = match(X, U, ctc, X.device)
+            xfeat = features(Xres, stt, amps)
+            if ibatch == 0:
+                neg = (stt[:, 0] - nt - nt // 2 + ops["nt0min"]) < 0
+                stt = stt[~neg, :]
+                xfeat = xfeat[~neg]
+                amps = amps[~neg, :]
+                th_amps = th_amps[~neg, :]
+            nsp = len(stt)
+            while k + nsp > st.shape[0]:
+                st = np.concatenate((st, np.zeros_like(st)), 0)
+                tF = torch.cat((tF, torch.zeros_like(tF)), 0)
+            t_shift = ibatch * bfile.batch_downsampling * (ops["batch_size"])
+            stt = stt.double()
+            st[k:k + nsp, 0] = ((stt[:, 0] - nt) + t_shift).cpu().numpy() - nt // 2 + ops["nt0min"]
+            st[k:k + nsp, 1] = stt[:, 1].cpu().numpy()
+            st[k:k + nsp, 2] = th_amps.cpu().numpy().squeeze(-1)
+            tF[k:k + nsp] = xfeat.cpu()
+            k += nsp
+            if progress_bar is not None:
+                progress_bar.emit(int((ibatch + 1) / bfile.n_batches * 100))
+    except Exception:
+        logger.exception(f"Error in kilosort_b200.extract on batch {ibatch}")
+        raise
+    return st[:k], tF[:k]
+
+
+def sort_spikes(st, tF):
+    """The final ordering of kilosort/template_matching.py:122-124 (numpy's
+    default argsort of the times, as the reference calls it)."""
+    isort = np.argsort(st[:, 0])
+    return st[isort], tF[isort]
+
+
 def extract(ops, bfile, U, device=torch.device("cuda"), progress_bar=None):
     """Match every batch of ``bfile`` and collect spikes and PC features.
 
@@ -353,10 +423,6 @@ def extract(ops, bfile, U, device=torch.device("cuda"), progress_bar=None):
     tensor, ops)`` sorted by time, and stores ``iCC``, ``iCC_mask``, ``iU``
     in ``ops``.
     """
-    try:
-        from tqdm import tqdm
-    except ImportError:  # pragma: no cover
-        tqdm = None
     nC = ops["settings"]["nearest_chans"]
     position_limit = ops["settings"]["position_limit"]
     iCC, iCC_mask, iU, Ucc = prepare_extract(ops["xc"], ops["yc"], U, nC,
@@ -364,49 +430,13 @@ def extract(ops, bfile, U, device=torch.device("cuda"), progress_bar=None):
     ops["iCC"] = iCC
     ops["iCC_mask"] = iCC_mask
     ops["iU"] = iU
-    nt = ops["nt"]
     ctc = prepare_matching(ops, U)
-    st = np.zeros((10 ** 6, 3), "float64")
-    tF = torch.zeros((10 ** 6, nC, ops["settings"]["n_pcs"]))
-    k = 0
-    batches = np.arange(bfile.n_batches, dtype=np.int64)
-    prog = tqdm(batches, miniters=200 if progress_bar else None,
-                mininterval=60 if progress_bar else None) if tqdm else batches
     W = ops["wPCA"].contiguous()
     iCCd = iCC.to(U.device).contiguous()
-    ibatch = -1
-    try:
-        for ibatch in prog:
-            if ibatch % 100 == 0 and torch.cuda.is_available():
-                logger.debug(f"Batch {ibatch}: {torch.cuda.memory_allocated() / 2**30:.2f} GiB allocated")
-            X = bfile.padded_batch_to_torch(ibatch, ops)
-            stt, amps, th_amps, Xres = run_matching(ops, X, U, ctc, device=device)
-            xfeat = spike_features(Xres, stt, amps, W, iCCd, iU, Ucc)   # [N, nC, P]
-            if ibatch == 0:
-                neg = (stt[:, 0] - nt - nt // 2 + ops["nt0min"]) < 0
-                stt = stt[~neg, :]
-                xfeat = xfeat[~neg]
-                amps = amps[~neg, :]
-                th_amps = th_amps[~neg, :]
-            nsp = len(stt)
-            if k + nsp > st.shape[0]:
-                st = np.concatenate((st, np.zeros_like(st)), 0)
-                tF = torch.cat((tF, torch.zeros_like(tF)), 0)
-            t_shift = ibatch * bfile.batch_downsampling * (ops["batch_size"])
-            stt = stt.double()
-            st[k:k + nsp, 0] = ((stt[:, 0] - nt) + t_shift).cpu().numpy() - nt // 2 + ops["nt0min"]
-            st[k:k + nsp, 1] = stt[:, 1].cpu().numpy()
-            st[k:k + nsp, 2] = th_amps.cpu().numpy().squeeze()
-            tF[k:k + nsp] = xfeat.cpu()
-            k += nsp
-            if progress_bar is not None:
-                progress_bar.emit(int((ibatch + 1) / bfile.n_batches * 100))
-    except Exception:
-        logger.exception(f"Error in kilosort_b200.extract on batch {ibatch}")
-        raise
-    isort = np.argsort(st[:k, 0])
-    st = st[isort]
-    tF = tF[isort]
+    match, features = _match_features(ops, W, iCCd, iU, Ucc)
+    batches = np.arange(bfile.n_batches, dtype=np.int64)
+    st, tF = extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar)
+    st, tF = sort_spikes(st, tF)
     return st, tF, ops
 
 
