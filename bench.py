@@ -3,13 +3,18 @@
 
 Workload: C=384 channels (Neuropixels-1.0-like geometry), K=600 templates,
 20 batches of 60000 samples (+2*61 padding), nt=61, n_pcs=6, Th_learned=8,
-seeded synthetic data (kilosort_b200.synth, seed 1002).  A step is one pass of
-`run_matching` over all 20 batches with X resident in HBM (1.85 GB per step,
-larger than L2).  `value` is channel-samples/s of the split-BF16 projection
-form; the plain-FP32 form is timed in the same run.  `e2e` runs the same
-workload through the public `run_matching` from pinned host memory, with the
-host->device copy of X and the device->host copy of the spikes inside the
+seeded synthetic data (kilosort_b200.synth, seed 1002).  A step is one pass
+over all 20 batches with X resident in HBM (1.85 GB per step, larger than L2).
+Three forms are timed: `run_matching` per batch with the plain-FP32 and with
+the split-BF16 projection, and the batched split form (every batch in one
+captured graph: grouped tensor-core contraction, one cooperative peel launch
+split into autotuned teams, one residual launch).  `value` is channel-samples/s
+of the batched split form.  `e2e` runs that form from pinned host memory, with
+the host->device copy of X and the device->host copy of the spikes inside the
 timed region.
+
+    python bench.py --workload uneven     # three recordings, 200 uneven batches
+    python bench.py --workload adjoint    # reconstruction loss + adjoint
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -411,9 +416,36 @@ def main():
 
     sampler = ClockSampler(local)
     results = {}
+    batched = "bf16x3" in forms
     for form in forms:
-        ms, nsp = timed(device_step, form, sampler if form == head else None)
+        ms, nsp = timed(device_step, form,
+                        sampler if (form == head and not batched) else None)
         results[form] = dict(ms=ms, spikes=nsp)
+
+    # the batched split form: all batches in one captured graph (grouped
+    # tensor-core contraction, one cooperative peel launch split into teams,
+    # one residual launch), teams autotuned; inputs resident as above
+    matcher, teams, groups = None, None, None
+    if batched:
+        from kilosort_b200.batched import BatchedMatcher, Recording, autotune_schedule
+        mrec = Recording.from_ops(ops, U, ctc)
+        items = [(X, 0) for X in Xs]
+        teams, groups = autotune_schedule([mrec], items, "bf16x3", teams=(5, 10, 20),
+                                          groups=(1, 2, 4, 5))
+        matcher = BatchedMatcher([mrec], [(L, 0)] * len(Xs), "bf16x3", teams=teams,
+                                 graph=True, groups=groups)
+        for dst, X in zip(matcher.X, Xs):
+            dst.copy_(X)
+
+        def batched_step(form, spikes):
+            matcher.launch()
+            spikes.append(0)      # counted once after timing (reading them syncs)
+
+        ms_b, _ = timed(batched_step, "bf16x3_batched", sampler)
+        results["bf16x3_batched"] = dict(ms=ms_b,
+                                         spikes=sum(len(r[0]) for r in matcher.results()))
+        forms.append("bf16x3_batched")
+        head = "bf16x3_batched"
 
     # end to end from pinned host memory through the public API
     h2d = C * L * 4 * args.batches
@@ -431,7 +463,19 @@ def main():
             d2h[0] += st_h.numel() * 8 + a_h.numel() * 4 + t_h.numel() * 4
         spikes.append(n)
 
-    e2e_ms, _ = timed(e2e_step, head)
+    def e2e_batched(form, spikes):
+        for dst, Xhost in zip(matcher.X, Xh):
+            dst.copy_(Xhost, non_blocking=True)
+        matcher.launch()
+        n = 0
+        d2h[0] = 0
+        for st, amps, th, _ in matcher.results():
+            st_h, a_h, t_h = st.cpu(), amps.cpu(), th.cpu()
+            n += len(st_h)
+            d2h[0] += st_h.numel() * 8 + a_h.numel() * 4 + t_h.numel() * 4
+        spikes.append(n)
+
+    e2e_ms, _ = timed(e2e_batched if matcher is not None else e2e_step, head)
 
     # per-kernel breakdown of one pass through the public run_matching, timed
     # by events the library records inside the call (ks_trace_stages): energy
@@ -443,7 +487,8 @@ def main():
     stage = {"energy": 0.0, "project": 0.0, "peel": 0.0, "residual": 0.0}
     stage_batches = {k: [] for k in stage}
     kused, nsp_total = 0, 0
-    o_head = dict(ops, projection=head)
+    proj_head = "bf16x3" if "bf16x3" in results else "fp32"
+    o_head = dict(ops, projection=proj_head)
     for pass_ in range(2):
         for X in Xs:
             st, amps, th, _ = kb.run_matching(o_head, X, U, ctc, device=dev)
@@ -455,6 +500,12 @@ def main():
                 stage_batches[key].append(round(v, 3))
             kused += len(torch.unique(st[:, 1]))
             nsp_total += len(st)
+    batched_stage = None
+    if matcher is not None:
+        matcher.launch_eager()
+        _lib.check(lib.ks_trace_read(ms4, 4), "ks_trace_read")
+        batched_stage = dict(zip(("setup", "project", "peel", "residual"),
+                                 (round(v, 3) for v in ms4)))
     _lib.check(lib.ks_trace_stages(0), "ks_trace_stages")
     nb = args.batches
     hbm, bf16, peak_kind = peaks()
@@ -471,7 +522,19 @@ def main():
     peel_gbs = bytes_peel / (stage["peel"] * 1e-3) / 1e9
     fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
     traffic = PEEL_TRAFFIC_BYTES if (C, K, NT_BATCH) == (384, 600, 60000) else None
-    if stage["peel"] >= stage["project"]:
+    if batched_stage is not None and head == "bf16x3_batched":
+        # one peel_multi_kernel launch covers all batches of the step; its
+        # traffic is the per-batch ncu figure times the batches (same sizes)
+        t_b = batched_stage["peel"] * 1e-3
+        roof = {"kernel": "peel_multi_kernel", "bound": "hbm",
+                "achieved": bytes_peel / t_b / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": bytes_peel / t_b / 1e9 / hbm,
+                "traffic": traffic * nb if traffic else None, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": bytes_peel,
+                "no_reuse_bytes_per_launch": bytes_noreuse,
+                "traffic_gbs": (traffic * nb / t_b / 1e9 if traffic else None),
+                "ms_per_launch": batched_stage["peel"], "batches_per_launch": nb}
+    elif stage["peel"] >= stage["project"]:
         roof = {"kernel": "peel_kernel", "bound": "hbm", "achieved": peel_gbs, "peak": hbm,
                 "unit": "GB/s", "frac": peel_gbs / hbm, "traffic": traffic,
                 "peak_source": peak_kind,
@@ -480,7 +543,7 @@ def main():
                 "traffic_gbs": (traffic / (stage["peel"] / nb * 1e-3) / 1e9
                                 if traffic else None),
                 "ms_per_launch": stage["peel"] / nb}
-    elif head == "bf16x3":
+    elif proj_head == "bf16x3":
         roof = {"kernel": "project_bf16x3", "bound": "tensor", "achieved": proj_tflops,
                 "peak": bf16, "unit": "TFLOP/s", "frac": proj_tflops / bf16, "traffic": None,
                 "peak_source": peak_kind}
@@ -497,7 +560,12 @@ def main():
         cpu = {"value": C * NT_BATCH / dt, "unit": "channel-samples/s", "cores": threads,
                "kind": "port", "sample": "batch 0 (C=384, 60000 samples), oracle run_matching"}
         for form in forms:
-            st, amps, _, _ = kb.run_matching(dict(ops, projection=form), Xs[0], U, ctc, device=dev)
+            if form == "bf16x3_batched":
+                matcher.launch()
+                st, amps, _, _ = matcher.results()[0]
+            else:
+                st, amps, _, _ = kb.run_matching(dict(ops, projection=form), Xs[0], U, ctc,
+                                                 device=dev)
             a = agreement(st.cpu().numpy(), st_r, amps.cpu().numpy(), amps_r)
             agr[form] = {k: a[k] for k in ("agreement", "amp_rel_max", "matched", "n_a", "n_r")}
 
@@ -511,6 +579,8 @@ def main():
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": head_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if head == "fp32" else "f32 (split-bf16 projection)",
+        # value/ms_per_step/e2e: the head form (the batched split form when
+        # the tensor-core build is present); forms lists every form timed
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "projection": head, "batches": nb,
                    "l2": "inputs larger than L2 (1.85 GB of X per step)",
@@ -521,8 +591,13 @@ def main():
                       "spikes_per_step": r["spikes"]} for f, r in results.items()},
         "speedup_split_vs_fp32": (results["fp32"]["ms"] / results["bf16x3"]["ms"]
                                   if "bf16x3" in results else None),
+        "speedup_batched_split_vs_fp32": (results["fp32"]["ms"] / results[head]["ms"]
+                                          if head == "bf16x3_batched" else None),
+        "batched_teams": teams,
+        "batched_groups": groups if matcher is not None else None,
         "stages_ms_per_step": stage,
         "stages_ms_per_batch": stage_batches,
+        "batched_stages_ms_per_step": batched_stage,
         "agreement_vs_oracle_batch0": agr,
         "e2e": {"value": per_step_samples * world / (e2e_ms * 1e-3), "unit": "channel-samples/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h[0],
@@ -535,7 +610,9 @@ def main():
                                       "algorithmic_bytes": bytes_res}},
         "cpu_baseline": cpu,
         "clocks": sampler.summary(),
-        "gpu_launches": launches_per_batch * nb,
+        # batched head: energy, {nm, 1/nm}, reorder, a temporal projection per
+        # batch, grouped contraction, peel, residual
+        "gpu_launches": (3 + nb + 3) if head == "bf16x3_batched" else launches_per_batch * nb,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

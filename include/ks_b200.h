@@ -192,12 +192,18 @@ KS_API int ks_peel_static(float* Bt, float* Xres, const float* U, const float* W
  * contraction of every batch (split-BF16: one grouped tensor-core launch;
  * FP32: one launch per batch); one cooperative peel launch whose grid is split
  * into `teams` groups of co-resident blocks, each peeling its share of the
- * batches (longest first) with no host round trip; one residual launch for all
- * batches.  teams <= 0 picks a default.  info[1] of a batch that no team
- * reached (after an error) stays -1.  Nothing is copied from host memory and
- * the host is not synchronised, so the call can be captured in a CUDA graph
- * (the descriptors are read at call time).  ctcT is the transposed layout
- * (KS_CTC_KJL).  Xres may equal X (in place); otherwise they must not overlap.
+ * batches (longest first) and then applying that batch's residual, with no
+ * host round trip.  teams <= 0 picks a default.  With an aux_stream other
+ * than stream and groups > 1 the batches (longest first) are split into
+ * `groups` consecutive groups: the projections of group g+1 run on
+ * aux_stream while group g is peeled on stream (the peel then runs one block
+ * per SM, leaving room for the projection kernels); stream waits for
+ * aux_stream before returning control of the work to the caller's later
+ * launches.  info[1] of a batch that no team reached (after an error) stays
+ * -1.  Nothing is copied from host memory and the host is not synchronised,
+ * so the call can be captured in a CUDA graph (the descriptors are read at
+ * call time).  ctcT is the transposed layout (KS_CTC_KJL).  Xres may equal X
+ * (in place); otherwise they must not overlap.
  */
 #define KS_MAX_BATCHES 256
 #define KS_MAX_RECORDINGS 8
@@ -226,8 +232,9 @@ KS_API size_t ks_match_batches_workspace_size(const ks_rec_desc* recs, int64_t n
                                               int64_t teams);
 KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
                             const ks_batch_desc* batches, int64_t n_batches,
-                            int precision, int64_t teams, void* workspace,
-                            size_t workspace_bytes, void* stream);
+                            int precision, int64_t teams, int64_t groups,
+                            void* workspace, size_t workspace_bytes, void* stream,
+                            void* aux_stream);
 
 /*
  * Fixed-assignment reconstruction loss and its adjoint, for template
@@ -266,7 +273,9 @@ KS_API int ks_recon_adjoint(const float* Xres, const int64_t* st, const float* a
  * after the template energies, after the projection, after the peel kernel,
  * after the residual kernel.  ks_trace_read waits for the last of the first
  * n+1 events of the thread's most recent traced call and writes n <= 4
- * intervals in ms: [energy + copy, projection, peel kernel, residual].  The
+ * intervals in ms: [energy + copy, projection, peel kernel, residual]
+ * (ks_match_batches records the same five points around its stages:
+ * [per-recording set-up, projections, peel launch, residual launch]).  The
  * events are the library's, created on the current device by the first
  * ks_trace_stages(1).  No reference counterpart (the reference has no
  * tracing of this path).

@@ -68,7 +68,7 @@ SIGNATURES = {
     "ks_trace_stages": (_int, [_int]),
     "ks_trace_read": (_int, [_vp, _int]),
     "ks_match_batches_workspace_size": (_sz, [_vp, _i64, _vp, _i64, _int, _i64]),
-    "ks_match_batches": (_int, [_vp, _i64, _vp, _i64, _int, _i64, _vp, _sz, _vp]),
+    "ks_match_batches": (_int, [_vp, _i64, _vp, _i64, _int, _i64, _i64, _vp, _sz, _vp, _vp]),
 }
 
 KS_MAX_BATCHES = 256

@@ -13,7 +13,8 @@ residual launch.  Each batch gets exactly what ``run_matching`` returns for it.
 * ``BatchedMatcher`` fixed shapes: preallocated inputs, outputs and workspace,
                      optionally captured once in a CUDA graph and replayed
 * ``autotune_teams`` times candidate team counts on the device and caches the
-                     fastest per workload signature
+                     fastest per workload signature; ``autotune_schedule``
+                     also picks the number of pipelined groups
 """
 from __future__ import annotations
 
@@ -122,12 +123,14 @@ def workspace_size(recs, items, projection="bf16x3", teams=0) -> int:
     return n
 
 
-def _launch(recs, items, outs, info, ws, projection, teams):
+def _launch(recs, items, outs, info, ws, projection, teams, groups=1, aux=None):
     rd, bd = _descs(recs, items, outs, info)
     lib = _lib.load()
     _lib.check(lib.ks_match_batches(C.byref(rd), len(recs), C.byref(bd), len(items),
-                                    _PROJECTIONS[projection], int(teams), _ptr(ws), ws.numel(),
-                                    _stream(ws.device)), "ks_match_batches")
+                                    _PROJECTIONS[projection], int(teams), int(groups),
+                                    _ptr(ws), ws.numel(), _stream(ws.device),
+                                    aux.cuda_stream if (aux is not None and groups > 1) else None),
+               "ks_match_batches")
 
 
 def _results(outs, info, what="ks_match_batches"):
@@ -145,12 +148,14 @@ def _results(outs, info, what="ks_match_batches"):
 
 
 def match_batches(recs: Sequence[Recording], items: Sequence[Tuple[torch.Tensor, int]],
-                  projection: str = "bf16x3", teams: int = 0):
+                  projection: str = "bf16x3", teams: int = 0, groups: int = 1):
     """Match every ``(X, recording index)`` of ``items``.
 
     Returns a list of ``(st, amps, th_amps, Xres)``, one per batch, equal to
     what ``run_matching`` returns for that batch alone.  Groups larger than
-    256 batches are split into consecutive calls.
+    256 batches are split into consecutive calls.  ``groups`` > 1 pipelines
+    the projections of one group of batches with the peel of the previous
+    one on a second stream.
     """
     recs = list(recs)
     items = [(_need(X, "X", ndim=2), int(r)) for X, r in items]
@@ -162,7 +167,8 @@ def match_batches(recs: Sequence[Recording], items: Sequence[Tuple[torch.Tensor,
         info = torch.empty((len(grp), 4), dtype=torch.int64, device=dev)
         ws = torch.empty(workspace_size(recs, grp, projection, teams), dtype=torch.uint8,
                          device=dev)
-        _launch(recs, grp, outs, info, ws, projection, teams)
+        aux = torch.cuda.Stream(dev) if groups > 1 else None
+        _launch(recs, grp, outs, info, ws, projection, teams, groups, aux)
         out.extend(_results(outs, info))
     return out
 
@@ -180,7 +186,7 @@ def _signature(recs, lengths_recs, projection):
 
 def autotune_teams(recs: Sequence[Recording], items: Sequence[Tuple[torch.Tensor, int]],
                    projection: str = "bf16x3", candidates=(1, 2, 4, 8, 16, 32),
-                   reps: int = 2) -> int:
+                   reps: int = 2, groups: int = 1) -> int:
     """Fastest team count for this workload, timed with CUDA events.
 
     Every candidate runs the full call (warm-up once, then ``reps`` timed
@@ -189,7 +195,7 @@ def autotune_teams(recs: Sequence[Recording], items: Sequence[Tuple[torch.Tensor
     """
     recs = list(recs)
     items = [(_need(X, "X", ndim=2), int(r)) for X, r in items]
-    key = _signature(recs, [(X.shape[1], r) for X, r in items], projection)
+    key = _signature(recs, [(X.shape[1], r) for X, r in items], projection) + (groups,)
     if key in _TEAMS_CACHE:
         return _TEAMS_CACHE[key]
     dev = _check_group(recs, items)
@@ -199,13 +205,14 @@ def autotune_teams(recs: Sequence[Recording], items: Sequence[Tuple[torch.Tensor
     ws = torch.empty(max(workspace_size(recs, items, projection, t) for t in cands),
                      dtype=torch.uint8, device=dev)
     best, best_ms = cands[0], float("inf")
+    aux = torch.cuda.Stream(dev) if groups > 1 else None
     for t in cands:
-        _launch(recs, items, outs, info, ws, projection, t)
+        _launch(recs, items, outs, info, ws, projection, t, groups, aux)
         _results(outs, info, "autotune_teams")
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(reps):
-            _launch(recs, items, outs, info, ws, projection, t)
+            _launch(recs, items, outs, info, ws, projection, t, groups, aux)
         e1.record()
         torch.cuda.synchronize(dev)
         _results(outs, info, "autotune_teams")
@@ -214,6 +221,40 @@ def autotune_teams(recs: Sequence[Recording], items: Sequence[Tuple[torch.Tensor
             best, best_ms = t, ms
     _TEAMS_CACHE[key] = best
     return best
+
+
+def autotune_schedule(recs: Sequence[Recording], items: Sequence[Tuple[torch.Tensor, int]],
+                      projection: str = "bf16x3", teams=(4, 8, 16, 20), groups=(1, 2, 4),
+                      reps: int = 2) -> Tuple[int, int]:
+    """Fastest (teams, groups) pair: teams tuned per group count, then the
+    group counts compared on their best team count (CUDA-event timing)."""
+    best = None
+    for g in groups:
+        if g > len(items):
+            continue
+        t = autotune_teams(recs, items, projection, candidates=teams, reps=reps, groups=g)
+        ms = _time_schedule(recs, items, projection, t, g, reps)
+        if best is None or ms < best[0]:
+            best = (ms, t, g)
+    return best[1], best[2]
+
+
+def _time_schedule(recs, items, projection, teams, groups, reps):
+    items = [(_need(X, "X", ndim=2), int(r)) for X, r in items]
+    dev = _check_group(list(recs), items)
+    outs = [_Outputs(recs[r], X.shape[0], X.shape[1], dev) for X, r in items]
+    info = torch.empty((len(items), 4), dtype=torch.int64, device=dev)
+    ws = torch.empty(workspace_size(recs, items, projection, teams), dtype=torch.uint8, device=dev)
+    aux = torch.cuda.Stream(dev) if groups > 1 else None
+    _launch(recs, items, outs, info, ws, projection, teams, groups, aux)
+    _results(outs, info, "autotune_schedule")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        _launch(recs, items, outs, info, ws, projection, teams, groups, aux)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1) / reps
 
 
 # ------------------------------------------------------------------ fixed shapes
@@ -229,7 +270,8 @@ class BatchedMatcher:
 
     def __init__(self, recs: Sequence[Recording], lengths: Sequence[Tuple[int, int]],
                  projection: str = "bf16x3", teams: Optional[int] = 0, graph: bool = True,
-                 in_place: bool = False, workspace: Optional[torch.Tensor] = None):
+                 in_place: bool = False, workspace: Optional[torch.Tensor] = None,
+                 groups: int = 1):
         if projection not in _PROJECTIONS:
             raise ValueError(f"projection must be one of {sorted(_PROJECTIONS)}")
         if len(lengths) > _lib.KS_MAX_BATCHES:
@@ -247,6 +289,8 @@ class BatchedMatcher:
                               Xres=X if in_place else None) for X, r in self.items]
         self.info = torch.empty((len(self.items), 4), dtype=torch.int64, device=dev)
         self.teams = teams
+        self.groups = max(1, int(groups))
+        self._aux = torch.cuda.Stream(dev) if self.groups > 1 else None
         # matchers whose launches never overlap (one stream) may share one
         # workspace of the largest size they need (workspace_bytes())
         self._ws = workspace
@@ -258,7 +302,8 @@ class BatchedMatcher:
 
     def _prepare(self):
         if self.teams is None:
-            self.teams = autotune_teams(self.recs, self.items, self.projection)
+            self.teams = autotune_teams(self.recs, self.items, self.projection,
+                                        groups=self.groups)
         need = workspace_size(self.recs, self.items, self.projection, self.teams)
         if self._ws is None:
             self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
@@ -270,8 +315,7 @@ class BatchedMatcher:
         self._prepare()
         if self.graph_enabled:
             if self._graph is None:
-                _launch(self.recs, self.items, self.outs, self.info, self._ws, self.projection,
-                        self.teams)                # warm-up: first-use set-up out of capture
+                self._enqueue()                    # warm-up: first-use set-up out of capture
                 torch.cuda.synchronize(self.device)
                 g = torch.cuda.CUDAGraph()
                 s = torch.cuda.Stream(self.device)
@@ -279,16 +323,23 @@ class BatchedMatcher:
                 with torch.cuda.stream(s):
                     g.capture_begin(capture_error_mode="thread_local")
                     try:
-                        _launch(self.recs, self.items, self.outs, self.info, self._ws,
-                                self.projection, self.teams)
+                        self._enqueue()
                     finally:
                         g.capture_end()
                 torch.cuda.current_stream(self.device).wait_stream(s)
                 self._graph = g
             self._graph.replay()
         else:
-            _launch(self.recs, self.items, self.outs, self.info, self._ws, self.projection,
-                    self.teams)
+            self._enqueue()
+
+    def _enqueue(self):
+        _launch(self.recs, self.items, self.outs, self.info, self._ws, self.projection,
+                self.teams, self.groups, self._aux)
+
+    def launch_eager(self):
+        """Enqueue one pass without the graph (for stage tracing or debugging)."""
+        self._prepare()
+        self._enqueue()
 
     def results(self):
         """Per batch ``(st, amps, th_amps, Xres)`` (synchronises to read the status).

@@ -129,8 +129,11 @@ ks_recon_kernel(const float* __restrict__ X, const long long* __restrict__ st,
                 const float* __restrict__ W, const int* __restrict__ off,
                 const int* __restrict__ idx, int C, int L, int K, int P, int nt, int nblk,
                 int ngrp, float* __restrict__ Xres, double* __restrict__ part) {
-  extern __shared__ float sW[];   // [P][nt]
-  for (int i = threadIdx.x; i < P * nt; i += blockDim.x) sW[i] = W[i];
+  extern __shared__ __align__(16) float sW[];   // Wt[t][8], components padded to 8
+  for (int i = threadIdx.x; i < 8 * nt; i += blockDim.x) {
+    const int t = i >> 3, p = i & 7;
+    sW[i] = p < P ? W[p * nt + t] : 0.f;
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const long long w = (long long)blockIdx.x * (kRecThreads / 32) + (threadIdx.x >> 5);
@@ -171,14 +174,17 @@ ks_recon_kernel(const float* __restrict__ X, const long long* __restrict__ st,
         for (int pp = 0; pp < 8; ++pp)
           u[pp] = (chok && pp < P) ? __ldg(U + ((long long)k * P + pp) * C + c) : 0.f;
         const int tt0 = c0 - tau + half;
+        const float4* W4 = reinterpret_cast<const float4*>(sW);
 #pragma unroll
         for (int j = 0; j < kCol; ++j) {
           const int t = tt0 + j;
           if (t >= 0 && t < nt) {
+            const float4 wa = W4[2 * t], wb = W4[2 * t + 1];
+            const float wt[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
             float wv = 0.f;
 #pragma unroll
             for (int pp = 0; pp < 8; ++pp)
-              if (pp < P) wv = fmaf(u[pp], sW[pp * nt + t], wv);
+              if (pp < P) wv = fmaf(u[pp], wt[pp], wv);
             x[j] = __fsub_rn(x[j], __fmul_rn(amp, wv));
           }
         }
@@ -396,7 +402,7 @@ extern "C" KS_API int ks_recon_loss(const float* X, const int64_t* st, const flo
     KS_CUDA(cudaGetLastError());
   }
   const unsigned grid = (unsigned)((r.nwarps + kRecThreads / 32 - 1) / (kRecThreads / 32));
-  ks_recon_kernel<<<grid, kRecThreads, sizeof(float) * P * nt, s>>>(
+  ks_recon_kernel<<<grid, kRecThreads, sizeof(float) * 8 * nt, s>>>(
       X, stp, amps, U, W, off, idx, (int)C, (int)L, (int)K, (int)P, (int)nt, (int)r.nblk,
       (int)r.ngrp, Xres, part);
   KS_CUDA(cudaGetLastError());

@@ -66,6 +66,7 @@ struct MultiParams {
   size_t team_bytes;
   unsigned long long limit_ns;
   const int* upstream_err;
+  size_t peel_smem;             // dynamic shared bytes of the peel (lists follow)
 };
 
 __device__ void fill_args(const MultiParams& p, int b, char* team, PeelArgs& a) {
@@ -94,56 +95,72 @@ __device__ void fill_args(const MultiParams& p, int b, char* team, PeelArgs& a) 
   bind_scratch(a, team, mb.lists);
   a.limit_ns = p.limit_ns;
   a.upstream_err = p.upstream_err;
+#ifdef KS_PEEL_TRACE
+  a.trace = 1;
+#endif
 }
 
 // Team blockIdx.x / team_size peels its batches one after the other; the
-// team's barrier count carries over from batch to batch.  A team stops at its
-// first error (info of its later batches keeps the "not run" value).
+// team's barrier count carries over from batch to batch.  After a batch's
+// peel the same team applies its residual pass (record order per element, as
+// ks_residual_kernel does), so one team's residual work fills the barrier
+// waits of the others.  A team stops at its first error (info of its later
+// batches keeps the "not run" value).
+template <int kRows>
+__device__ __forceinline__ void peel_multi_body(const MultiParams& p, char* smem_raw,
+                                                PeelArgs& sa);
+
+// Alone on the device: 2 blocks per SM (64 registers per thread).
 __global__ void __launch_bounds__(kThreads, 2) peel_multi_kernel(const __grid_constant__ MultiParams p) {
   extern __shared__ __align__(16) char smem_raw[];
   __shared__ PeelArgs sa;
+  peel_multi_body<kRowsPerWarp>(p, smem_raw, sa);
+}
+
+// Beside the projection kernels of the next group: 1 block per SM capped at
+// 80 registers per thread (40960 of the SM's 65536), which leaves room for a
+// tensor-core contraction CTA (192 x 64) or a temporal-projection block
+// (256 x 80) on the same SM.
+__global__ void __maxnreg__(80) peel_multi_kernel_shared(const __grid_constant__ MultiParams p) {
+  extern __shared__ __align__(16) char smem_raw[];
+  __shared__ PeelArgs sa;
+  peel_multi_body<kRowsPerWarp>(p, smem_raw, sa);
+}
+
+template <int kRows>
+__device__ __forceinline__ void peel_multi_body(const MultiParams& p, char* smem_raw,
+                                                PeelArgs& sa) {
   const int team = blockIdx.x / p.team_size;
   const int rank = blockIdx.x % p.team_size;
   const int n_teams = gridDim.x / p.team_size;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   char* tbase = p.teams + (size_t)team * p.team_bytes;
+  // per-warp residual lists after the peel's own shared memory
+  int* xl = reinterpret_cast<int*>(smem_raw + p.peel_smem);
   unsigned epoch = 0;
   for (int i = team; i < p.n_batches; i += n_teams) {
     __syncthreads();
     if (threadIdx.x == 0) fill_args(p, p.order[i], tbase, sa);
     __syncthreads();
     const Smem s = carve_smem(sa, smem_raw);
-    run_peel(sa, s, rank, (unsigned)p.team_size, epoch);
-    // leave together: thread 0 reads the team's error word for the block
-    if (__syncthreads_or(threadIdx.x == 0 && ks_ld_volatile(sa.err) != 0)) break;
+    const PeelOutcome o = run_peel<kRows>(sa, s, rank, (unsigned)p.team_size, epoch);
+    if (o.status != KS_OK) {
+      if (o.status == KS_ERR_OVERFLOW) continue;   // that batch only
+      break;
+    }
+    if (o.n_out > 0) {
+      ResSmem rs;
+      rs.W = s.W;
+      rs.xl_tau = xl;
+      rs.xl_k = xl + kWarps * kXList;
+      rs.xl_amp = reinterpret_cast<float*>(xl + 2 * kWarps * kXList);
+      const int xg = (sa.C + 31) / 32;
+      const long long n_items = (long long)sa.nblk * xg;
+      for (long long w = (long long)rank * kWarps + warp; w < n_items;
+           w += (long long)p.team_size * kWarps)
+        residual_item(sa, rs, o.iters, o.n_out, (int)(w / xg), (int)(w % xg), lane, warp);
+    }
   }
-}
-
-// Residual pass of every batch: blockIdx.y is the batch.
-__global__ void __launch_bounds__(kResThreads) residual_multi_kernel(const __grid_constant__ MultiParams p) {
-  extern __shared__ __align__(16) char smem_raw[];
-  __shared__ PeelArgs sa;
-  const int b = blockIdx.y;
-  if (threadIdx.x == 0) fill_args(p, b, p.teams, sa);
-  __syncthreads();
-  float* sW = reinterpret_cast<float*>(smem_raw);
-  const int wn = (sa.P * sa.nt + 3) & ~3;
-  ResSmem s;
-  s.W = sW;
-  s.xl_tau = reinterpret_cast<int*>(sW + wn);
-  s.xl_k = s.xl_tau + kResWarps * kXList;
-  s.xl_amp = reinterpret_cast<float*>(s.xl_k + kResWarps * kXList);
-  for (int i = threadIdx.x; i < sa.P * sa.nt; i += kResThreads) sW[i] = sa.W[i];
-  __syncthreads();
-  const long long n_out = sa.info[0];
-  const int status = (int)sa.info[1];
-  const int n_iter = (int)sa.info[2];
-  if (status != KS_OK || n_out <= 0) return;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int xg = (sa.C + 31) / 32;
-  const long long n_items = (long long)sa.nblk * xg;
-  const long long w = (long long)blockIdx.x * kResWarps + warp;
-  if (w >= n_items) return;
-  residual_item(sa, s, n_iter, n_out, (int)(w / xg), (int)(w % xg), lane, warp);
 }
 
 // -------------------------------------------------------------- host layout
@@ -253,10 +270,40 @@ extern "C" KS_API size_t ks_match_batches_workspace_size(const ks_rec_desc* recs
   return pl.bytes;
 }
 
+namespace {
+
+// Events that order the projection stream and the peel stream of a pipelined
+// call (per host thread, created once, reused by every call).
+cudaEvent_t pipeline_event(int i) {
+  static thread_local std::vector<cudaEvent_t> ev;
+  while ((int)ev.size() <= i) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    ev.push_back(e);
+  }
+  return ev[i];
+}
+
+// Kernel and resident blocks per SM of the peel: alone on the device 2 blocks
+// per SM; pipelined 1 block per SM, which leaves room on every SM for a block
+// of the projection kernels of the next group.
+struct PeelVariant {
+  void (*kernel)(MultiParams);
+  int blocks_per_sm;
+};
+
+PeelVariant peel_variant(bool pipelined) {
+  if (pipelined) return PeelVariant{peel_multi_kernel_shared, 1};
+  return PeelVariant{peel_multi_kernel, 2};
+}
+
+}  // namespace
+
 extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
                                        const ks_batch_desc* batches, int64_t n_batches,
-                                       int precision, int64_t teams, void* workspace,
-                                       size_t workspace_bytes, void* stream) {
+                                       int precision, int64_t teams, int64_t groups,
+                                       void* workspace, size_t workspace_bytes, void* stream,
+                                       void* aux_stream) {
   using namespace ks;
   if (!recs || !batches) return fail(KS_ERR_ARG, "ks_match_batches: null descriptor array");
   Plan pl;
@@ -270,8 +317,13 @@ extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
   rc = device_info(&dev);
   if (rc) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStream_t ps = aux_stream ? static_cast<cudaStream_t>(aux_stream) : s;
+  const int G = (aux_stream && aux_stream != stream)
+                    ? (int)std::max<int64_t>(1, std::min<int64_t>(groups, n_batches)) : 1;
+  const bool pipelined = G > 1;
   char* base = static_cast<char*>(workspace);
   int* gemm_err = reinterpret_cast<int*>(base + pl.ctl);
+  trace_mark(0, s);
   KS_CUDA(cudaMemsetAsync(gemm_err, 0, sizeof(int), s));
 
   // per recording: nm, {nm, 1/nm}, reordered templates
@@ -290,68 +342,22 @@ extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
                                     reinterpret_cast<float*>(base + rp.uf), nullptr, nullptr, s);
     if (rc) return rc;
   }
-  // per batch: the residual starts as X; projections
-  for (int64_t b = 0; b < n_batches; ++b) {
-    const ks_batch_desc& d = batches[b];
-    const ks_rec_desc& r = recs[d.rec];
-    const RecPlan& rp = pl.rec[d.rec];
-    const BatchPlan& bp = pl.bat[b];
-    if (d.Xres != d.X)
-      KS_CUDA(cudaMemcpyAsync(d.Xres, d.X, sizeof(float) * r.C * d.L, cudaMemcpyDeviceToDevice, s));
-    KS_CUDA(cudaMemsetAsync(d.info, 0xff, 4 * sizeof(int64_t), s));   // "not run" until the peel writes it
-    float* Bt = reinterpret_cast<float*>(base + bp.bt);
-    if (precision == KS_PROJ_BF16X3) {
-      __nv_bfloat16* yhi = reinterpret_cast<__nv_bfloat16*>(base + rp.yhi) + (size_t)bp.row_off * rp.Q;
-      __nv_bfloat16* ylo = reinterpret_cast<__nv_bfloat16*>(base + rp.ylo) + (size_t)bp.row_off * rp.Q;
-      if ((rc = launch_temporal(d.X, r.W, r.C, d.L, r.P, r.nt, rp.Q, bp.Lpad, nullptr, yhi, ylo, s)))
-        return rc;
-    } else {
-      float* yf = reinterpret_cast<float*>(base + pl.yf);
-      if ((rc = launch_temporal(d.X, r.W, r.C, d.L, r.P, r.nt, rp.Q, bp.Lpad, yf, nullptr, nullptr, s)))
-        return rc;
-      if ((rc = sgemm_tn(reinterpret_cast<const float*>(base + rp.uf), yf, Bt, r.K, d.L, rp.Q, 0, s,
-                         true)))
-        return rc;
-    }
-  }
-  if (precision == KS_PROJ_BF16X3) {
-    static thread_local GemmGroup g;   // about 14 KB: kept off the stack
-    for (int64_t r = 0; r < n_recs; ++r) {
-      const RecPlan& rp = pl.rec[r];
-      g.nk[r] = (int)(rp.Q / 64);
-      if (rp.rows == 0) continue;
-      const __nv_bfloat16* uhi = reinterpret_cast<const __nv_bfloat16*>(base + rp.uhi);
-      const __nv_bfloat16* ulo = reinterpret_cast<const __nv_bfloat16*>(base + rp.ulo);
-      const __nv_bfloat16* yhi = reinterpret_cast<const __nv_bfloat16*>(base + rp.yhi);
-      const __nv_bfloat16* ylo = reinterpret_cast<const __nv_bfloat16*>(base + rp.ylo);
-      if ((rc = make_bf16_map(&g.maps[r][0], uhi, rp.Kpad, rp.Q, gemm_tile_m()))) return rc;
-      if ((rc = make_bf16_map(&g.maps[r][1], ulo, rp.Kpad, rp.Q, gemm_tile_m()))) return rc;
-      if ((rc = make_bf16_map(&g.maps[r][2], yhi, rp.rows, rp.Q, gemm_tile_n()))) return rc;
-      if ((rc = make_bf16_map(&g.maps[r][3], ylo, rp.rows, rp.Q, gemm_tile_n()))) return rc;
-    }
-    long long tiles = 0;
-    for (int64_t b = 0; b < n_batches; ++b) {
-      const ks_batch_desc& d = batches[b];
-      GemmBatch& gb = g.batches[b];
-      gb.B = reinterpret_cast<float*>(base + pl.bat[b].bt);
-      gb.ldb = 0;
-      gb.K = (int)recs[d.rec].K;
-      gb.L = (int)d.L;
-      gb.rec = (int)d.rec;
-      gb.row_off = (int)pl.bat[b].row_off;
-      gb.tiles_m = (int)(pl.rec[d.rec].Kpad / gemm_tile_m());
-      gb.tile_begin = (int)tiles;
-      tiles += (long long)gb.tiles_m * ((d.L + gemm_tile_n() - 1) / gemm_tile_n());
-    }
-    if (tiles > 0x7fffffffLL) return fail(KS_ERR_UNSUPPORTED, "ks_match_batches: too many tiles");
-    g.n_batches = (int)n_batches;
-    g.n_tiles = (int)tiles;
-    g.tiled = 1;
-    g.err = gemm_err;
-    if ((rc = launch_gemm_group(g, s))) return rc;
+  trace_mark(1, s);
+  if (pipelined) {
+    cudaEvent_t e = pipeline_event(0);
+    if (!e) return fail(KS_ERR_CUDA, "ks_match_batches: cudaEventCreate failed");
+    KS_CUDA(cudaEventRecord(e, s));
+    KS_CUDA(cudaStreamWaitEvent(ps, e, 0));
   }
 
-  // the peel of every batch: one cooperative launch of teams
+  // batches longest first; groups are consecutive runs of that order
+  std::vector<int> order(n_batches);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return batches[x].L * recs[batches[x].rec].K > batches[y].L * recs[batches[y].rec].K;
+  });
+
+  // batch table of the peel, shared by every group's launch
   static thread_local MultiParams mp;   // about 19 KB: kept off the stack
   for (int64_t r = 0; r < n_recs; ++r) {
     const ks_rec_desc& d = recs[r];
@@ -369,14 +375,7 @@ extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
     m.max_peels = (int)d.max_peels;
     m.capacity = d.capacity;
   }
-  std::vector<int> order(n_batches);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    return batches[x].L * recs[batches[x].rec].K > batches[y].L * recs[batches[y].rec].K;
-  });
   size_t smem = 0;
-  long long max_items = 0;
-  int maxP = 1, max_nt = 1;
   for (int64_t b = 0; b < n_batches; ++b) {
     const ks_batch_desc& d = batches[b];
     const ks_rec_desc& r = recs[d.rec];
@@ -390,49 +389,126 @@ extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
     m.lists = base + pl.bat[b].lists;
     m.L = (int)d.L;
     m.rec = (int)d.rec;
-    mp.order[b] = order[b];
     const int nchunks = (int)((d.L + kChunk - 1) / kChunk);
     const int nblk = (int)((d.L + kCol - 1) / kCol);
     const int nwords = (nblk + 31) / 32;
     smem = std::max(smem, smem_bytes((int)r.P, (int)r.nt, nchunks, nwords));
-    max_items = std::max<long long>(max_items, (long long)nblk * ((r.C + 31) / 32));
-    maxP = std::max<int>(maxP, (int)r.P);
-    max_nt = std::max<int>(max_nt, (int)r.nt);
   }
-  mp.n_batches = (int)n_batches;
   mp.teams = base + pl.teams;
   mp.team_bytes = pl.team_bytes;
   mp.limit_ns = wait_limit_ns();
   mp.upstream_err = precision == KS_PROJ_BF16X3 ? gemm_err : nullptr;
+  smem = (smem + 15) & ~size_t(15);
+  mp.peel_smem = smem;
+  smem += (size_t)kWarps * kXList * (2 * sizeof(int) + sizeof(float));   // residual lists
+  const PeelVariant pv = peel_variant(pipelined);
   cudaFuncAttributes fa;
-  KS_CUDA(cudaFuncGetAttributes(&fa, peel_multi_kernel));
+  KS_CUDA(cudaFuncGetAttributes(&fa, pv.kernel));
   if (smem + fa.sharedSizeBytes > dev.smem_optin)
     return fail(KS_ERR_UNSUPPORTED, "ks_match_batches: batch too long for shared memory");
-  KS_CUDA(cudaFuncSetAttribute(peel_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  KS_CUDA(cudaFuncSetAttribute(pv.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
-  KS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, peel_multi_kernel, kThreads, smem));
+  KS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pv.kernel, kThreads, smem));
   if (occ < 1) return fail(KS_ERR_UNSUPPORTED, "ks_match_batches: peel does not fit on an SM");
-  const int max_blocks = dev.sm_count * occ;
-  if (pl.n_teams > max_blocks) return fail(KS_ERR_UNSUPPORTED, "ks_match_batches: more teams than resident blocks");
-  mp.team_size = max_blocks / pl.n_teams;
-  const int grid = mp.team_size * pl.n_teams;
-  for (int t = 0; t < pl.n_teams; ++t)
-    KS_CUDA(cudaMemsetAsync(base + pl.teams + (size_t)t * pl.team_bytes, 0, 256, s));
-  cudaLaunchConfig_t cfg = {};
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeCooperative;
-  attr[0].val.cooperative = 1;
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  KS_CUDA(cudaLaunchKernelEx(&cfg, peel_multi_kernel, mp));
+  const int max_blocks = dev.sm_count * std::min(occ, pv.blocks_per_sm);
 
-  // residual of every batch
-  const dim3 rgrid((unsigned)((max_items + kResWarps - 1) / kResWarps), (unsigned)n_batches);
-  residual_multi_kernel<<<rgrid, kResThreads, residual_smem_bytes(maxP, max_nt), s>>>(mp);
-  KS_CUDA(cudaGetLastError());
+  static thread_local GemmGroup g;      // about 14 KB: kept off the stack
+  if (precision == KS_PROJ_BF16X3) {
+    for (int64_t r = 0; r < n_recs; ++r) {
+      const RecPlan& rp = pl.rec[r];
+      g.nk[r] = (int)(rp.Q / 64);
+      if (rp.rows == 0) continue;
+      const __nv_bfloat16* uhi = reinterpret_cast<const __nv_bfloat16*>(base + rp.uhi);
+      const __nv_bfloat16* ulo = reinterpret_cast<const __nv_bfloat16*>(base + rp.ulo);
+      const __nv_bfloat16* yhi = reinterpret_cast<const __nv_bfloat16*>(base + rp.yhi);
+      const __nv_bfloat16* ylo = reinterpret_cast<const __nv_bfloat16*>(base + rp.ylo);
+      if ((rc = make_bf16_map(&g.maps[r][0], uhi, rp.Kpad, rp.Q, gemm_tile_m()))) return rc;
+      if ((rc = make_bf16_map(&g.maps[r][1], ulo, rp.Kpad, rp.Q, gemm_tile_m()))) return rc;
+      if ((rc = make_bf16_map(&g.maps[r][2], yhi, rp.rows, rp.Q, gemm_tile_n()))) return rc;
+      if ((rc = make_bf16_map(&g.maps[r][3], ylo, rp.rows, rp.Q, gemm_tile_n()))) return rc;
+    }
+    g.tiled = 1;
+    g.err = gemm_err;
+  }
+
+  for (int gi = 0; gi < G; ++gi) {
+    const int i0 = (int)(n_batches * gi / G), i1 = (int)(n_batches * (gi + 1) / G);
+    // projections of the group's batches (on the projection stream)
+    for (int i = i0; i < i1; ++i) {
+      const int b = order[i];
+      const ks_batch_desc& d = batches[b];
+      const ks_rec_desc& r = recs[d.rec];
+      const RecPlan& rp = pl.rec[d.rec];
+      const BatchPlan& bp = pl.bat[b];
+      if (d.Xres != d.X)
+        KS_CUDA(cudaMemcpyAsync(d.Xres, d.X, sizeof(float) * r.C * d.L, cudaMemcpyDeviceToDevice, ps));
+      KS_CUDA(cudaMemsetAsync(d.info, 0xff, 4 * sizeof(int64_t), ps));   // "not run" until the peel writes it
+      float* Bt = reinterpret_cast<float*>(base + bp.bt);
+      if (precision == KS_PROJ_BF16X3) {
+        __nv_bfloat16* yhi = reinterpret_cast<__nv_bfloat16*>(base + rp.yhi) + (size_t)bp.row_off * rp.Q;
+        __nv_bfloat16* ylo = reinterpret_cast<__nv_bfloat16*>(base + rp.ylo) + (size_t)bp.row_off * rp.Q;
+        if ((rc = launch_temporal(d.X, r.W, r.C, d.L, r.P, r.nt, rp.Q, bp.Lpad, nullptr, yhi, ylo, ps)))
+          return rc;
+      } else {
+        float* yf = reinterpret_cast<float*>(base + pl.yf);
+        if ((rc = launch_temporal(d.X, r.W, r.C, d.L, r.P, r.nt, rp.Q, bp.Lpad, yf, nullptr, nullptr, ps)))
+          return rc;
+        if ((rc = sgemm_tn(reinterpret_cast<const float*>(base + rp.uf), yf, Bt, r.K, d.L, rp.Q, 0, ps,
+                           true)))
+          return rc;
+      }
+    }
+    if (precision == KS_PROJ_BF16X3) {
+      long long tiles = 0;
+      for (int i = i0; i < i1; ++i) {
+        const int b = order[i];
+        const ks_batch_desc& d = batches[b];
+        GemmBatch& gb = g.batches[i - i0];
+        gb.B = reinterpret_cast<float*>(base + pl.bat[b].bt);
+        gb.ldb = 0;
+        gb.K = (int)recs[d.rec].K;
+        gb.L = (int)d.L;
+        gb.rec = (int)d.rec;
+        gb.row_off = (int)pl.bat[b].row_off;
+        gb.tiles_m = (int)(pl.rec[d.rec].Kpad / gemm_tile_m());
+        gb.tile_begin = (int)tiles;
+        tiles += (long long)gb.tiles_m * ((d.L + gemm_tile_n() - 1) / gemm_tile_n());
+      }
+      if (tiles > 0x7fffffffLL) return fail(KS_ERR_UNSUPPORTED, "ks_match_batches: too many tiles");
+      g.n_batches = i1 - i0;
+      g.n_tiles = (int)tiles;
+      if ((rc = launch_gemm_group(g, ps))) return rc;
+    }
+    if (pipelined) {
+      cudaEvent_t e = pipeline_event(gi + 1);
+      if (!e) return fail(KS_ERR_CUDA, "ks_match_batches: cudaEventCreate failed");
+      KS_CUDA(cudaEventRecord(e, ps));
+      KS_CUDA(cudaStreamWaitEvent(s, e, 0));
+    }
+    if (gi == 0) trace_mark(2, s);
+    // the group's peels and residual passes: one cooperative launch of teams
+    const int nb = i1 - i0;
+    const int n_teams = std::min(pl.n_teams, nb);
+    if (n_teams > max_blocks) return fail(KS_ERR_UNSUPPORTED, "ks_match_batches: more teams than resident blocks");
+    for (int i = i0; i < i1; ++i) mp.order[i - i0] = order[i];
+    mp.n_batches = nb;
+    mp.team_size = max_blocks / n_teams;
+    for (int t = 0; t < n_teams; ++t)
+      KS_CUDA(cudaMemsetAsync(base + pl.teams + (size_t)t * pl.team_bytes, 0, 256, s));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.gridDim = dim3(mp.team_size * n_teams);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    KS_CUDA(cudaLaunchKernelEx(&cfg, pv.kernel, mp));
+  }
+  // the residual passes ran inside the peel launches
+  trace_mark(3, s);
+  trace_mark(4, s);
   return KS_OK;
 }

@@ -58,7 +58,7 @@ constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr int kChunk = 256;          // detection chunk, one column per thread
 constexpr int kCol = 32;             // update block, one column per lane
-constexpr int kRowsPerWarp = 16;     // template rows in flight per lane
+constexpr int kRowsPerWarp = 16;     // template rows in flight per lane (2 blocks per SM)
 constexpr int kItemRows = 64;        // template rows per update item (at most)
 constexpr int kTouch = 8;            // peaks touching one block (more: ties)
 constexpr int kMaxChunks = 16384;
@@ -138,7 +138,7 @@ struct PeelArgs {
 };
 
 struct Smem {
-  float* W;        // P*nt
+  float* W;        // Wt[nt][8] (the fused residual's basis)
   int* prefix;     // nchunks+1   exclusive prefix of chunk peak counts
   int* wprefix;    // nwords+1    exclusive prefix of dirty-bitmap popcounts
   float* win;      // kChunk + 2*nt   column scores around the chunk
@@ -151,6 +151,16 @@ struct Smem {
   float* tl_amp;   // kWarps*kTouch
 };
 
+// Wt[t][p] = W[p][t] for p < P, 0 for P <= p < 8: each tap's components are
+// two aligned float4 in shared memory.
+__device__ __forceinline__ void stage_basis_t8(const float* W, int P, int nt, float* sWt,
+                                               int nthreads) {
+  for (int i = threadIdx.x; i < 8 * nt; i += nthreads) {
+    const int t = i >> 3, p = i & 7;
+    sWt[i] = p < P ? W[p * nt + t] : 0.f;
+  }
+}
+
 __device__ __forceinline__ Smem carve_smem(const PeelArgs& a, char* base) {
   Smem s;
   size_t off = 0;
@@ -160,7 +170,7 @@ __device__ __forceinline__ Smem carve_smem(const PeelArgs& a, char* base) {
     return p;
   };
   const int wn = kChunk + 2 * a.nt;
-  s.W = reinterpret_cast<float*>(take(sizeof(float) * a.P * a.nt));
+  s.W = reinterpret_cast<float*>(take(sizeof(float) * 8 * a.nt));
   s.prefix = reinterpret_cast<int*>(take(sizeof(int) * (a.nchunks + 1)));
   s.wprefix = reinterpret_cast<int*>(take(sizeof(int) * (a.nwords + 1)));
   s.win = reinterpret_cast<float*>(take(sizeof(float) * wn));
@@ -177,7 +187,8 @@ __device__ __forceinline__ Smem carve_smem(const PeelArgs& a, char* base) {
 size_t smem_bytes(int P, int nt, int nchunks, int nwords) {
   auto r = [](size_t b) { return (b + 15) & ~size_t(15); };
   const size_t wn = kChunk + 2 * (size_t)nt;
-  return r(sizeof(float) * P * nt) + r(sizeof(int) * (nchunks + 1)) +
+  (void)P;
+  return r(sizeof(float) * 8 * nt) + r(sizeof(int) * (nchunks + 1)) +
          r(sizeof(int) * (nwords + 1)) + 3 * r(sizeof(float) * wn) +
          r(sizeof(int) * kChunk) + r(sizeof(int) * (kWarps + 1)) +
          3 * r(sizeof(int) * kWarps * kTouch);
@@ -432,6 +443,7 @@ __device__ __forceinline__ TouchList load_touch_warp(const PeelArgs& a, const Sm
 // rows of B (16 rows per round trip).  Later peaks of the same column (at
 // most one more unless scores tie exactly) are applied in a second round, in
 // the same order.
+template <int kRows>
 __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk,
                                  int j_lo, int j_hi, unsigned long long* pack_out,
                                  int lane) {
@@ -455,10 +467,10 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
   float* bcol = a.Bt + (size_t)blk * K * kCol + lane;
   float best = -1.f;
   int arg = 0;
-  for (int j0 = j_lo; j0 < j_hi; j0 += kRowsPerWarp) {
-    float bv[kRowsPerWarp], w0[kRowsPerWarp];
+  for (int j0 = j_lo; j0 < j_hi; j0 += kRows) {
+    float bv[kRows], w0[kRows];
 #pragma unroll
-    for (int r = 0; r < kRowsPerWarp; ++r) {
+    for (int r = 0; r < kRows; ++r) {
       const int j = j0 + r;
       const bool ok = colok && j < j_hi;
       bv[r] = ok ? bcol[(size_t)j * kCol] : 0.f;
@@ -466,7 +478,7 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
     }
     if (e0 >= 0) {
 #pragma unroll
-      for (int r = 0; r < kRowsPerWarp; ++r) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp0, w0[r]));
+      for (int r = 0; r < kRows; ++r) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp0, w0[r]));
     }
     if (any_rest) {
       for (int e = 0; e < tl.n; ++e) {
@@ -474,17 +486,17 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
           const float amp = tl.amp[e];
           const float* cp = a.ctcT + (size_t)tl.k[e] * K * nlag + (c - tl.tau[e] + nt);
 #pragma unroll
-          for (int r = 0; r < kRowsPerWarp; ++r) {
+          for (int r = 0; r < kRows; ++r) {
             const int j = j0 + r;
             w0[r] = (j < j_hi) ? __ldg(cp + (size_t)j * nlag) : 0.f;
           }
 #pragma unroll
-          for (int r = 0; r < kRowsPerWarp; ++r) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp, w0[r]));
+          for (int r = 0; r < kRows; ++r) bv[r] = __fsub_rn(bv[r], __fmul_rn(amp, w0[r]));
         }
       }
     }
 #pragma unroll
-    for (int r = 0; r < kRowsPerWarp; ++r) {
+    for (int r = 0; r < kRows; ++r) {
       const int j = j0 + r;
       if (colok && j < j_hi) {
         if (touched) bcol[(size_t)j * kCol] = bv[r];
@@ -509,17 +521,28 @@ __device__ __forceinline__ int dirty_block(const Smem& s, const unsigned* bits,
   return lo * 32 + bit;
 }
 
+// Outcome of one batch's peel, the same in every block of the team.
+struct PeelOutcome {
+  long long n_out;
+  int iters;
+  int status;
+};
+
 // The peel of one batch by a team of G co-resident blocks (this block has
 // rank `rank` in it); epoch is the team barrier's count of passed barriers,
 // carried across the batches a team processes.  The team first clears the
-// batch's per-run state, then runs the iterations; the outcome goes to info.
-__device__ void run_peel(const PeelArgs& a, const Smem& s, int rank, unsigned G,
-                         unsigned& epoch) {
+// batch's per-run state, then runs the iterations; the outcome goes to info
+// (written by one thread) and is returned to every thread.  When the status
+// is KS_OK every record and residual list of the batch is complete and
+// visible to the team (the last pass ended at a team barrier).
+template <int kRows>
+__device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsigned G,
+                                unsigned& epoch) {
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const long long gwarp = (long long)rank * kWarps + warp;
   const long long nwarps = (long long)G * kWarps;
-  for (int i = tid; i < a.P * a.nt; i += kThreads) s.W[i] = a.W[i];
+  stage_basis_t8(a.W, a.P, a.nt, s.W, kThreads);
   // a failed producer of the score matrix fails the peel
   if (rank == 0 && tid == 0 && a.upstream_err) {
     const int ue = ks_ld_volatile(a.upstream_err);
@@ -537,13 +560,14 @@ __device__ void run_peel(const PeelArgs& a, const Smem& s, int rank, unsigned G,
     if (t0 < 2) a.wctr[t0] = 0u;
   }
   if (!ks_grid_sync(a.bar, G, epoch, a.err, a.limit_ns)) {
+    const int e = ks_ld_volatile(a.err);
     if (rank == 0 && tid == 0) {
       a.info[0] = 0;
-      a.info[1] = ks_ld_volatile(a.err);
+      a.info[1] = e;
       a.info[2] = 0;
       a.info[3] = 0;
     }
-    return;
+    return PeelOutcome{0, 0, e ? e : KS_ERR_TIMEOUT};
   }
 
   // initial scores of every column, folded into pack[1]
@@ -554,7 +578,7 @@ __device__ void run_peel(const PeelArgs& a, const Smem& s, int rank, unsigned G,
     const long long n_items = (long long)a.nblk * rg;
     for (long long w = gwarp; w < n_items; w += nwarps) {
       const int blk = (int)(w / rg), r = (int)(w % rg);
-      update_warp_item(a, none, blk, r * kItemRows, min(a.K, (r + 1) * kItemRows), pinit, lane);
+      update_warp_item<kRows>(a, none, blk, r * kItemRows, min(a.K, (r + 1) * kItemRows), pinit, lane);
     }
   }
 
@@ -611,10 +635,10 @@ __device__ void run_peel(const PeelArgs& a, const Smem& s, int rank, unsigned G,
     int rows = kItemRows;
     if (ndirty > 0) {
       long long best_cost = -1;
-      for (int r = kRowsPerWarp; r <= kItemRows; r += kRowsPerWarp) {
+      for (int r = kRows; r <= kItemRows; r += kRows) {
         const long long items = (long long)ndirty * ((a.K + r - 1) / r);
         const long long per_warp = (items + nwarps - 1) / nwarps;
-        const long long cost = per_warp * (r / kRowsPerWarp + 1);
+        const long long cost = per_warp * (r / kRows + 1);
         if (best_cost < 0 || cost < best_cost) {
           best_cost = cost;
           rows = r;
@@ -637,7 +661,7 @@ __device__ void run_peel(const PeelArgs& a, const Smem& s, int rank, unsigned G,
       const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
       const int r = (int)(w % rgroups);
       const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
-      update_warp_item(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
+      update_warp_item<kRows>(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
     }
     while (true) {
       unsigned next = 0;
@@ -647,7 +671,7 @@ __device__ void run_peel(const PeelArgs& a, const Smem& s, int rank, unsigned G,
       const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
       const int r = (int)(w % rgroups);
       const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
-      update_warp_item(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
+      update_warp_item<kRows>(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
     }
     KS_TRACE(it, 4, ks_globaltimer());
     __syncthreads();
@@ -657,24 +681,26 @@ __device__ void run_peel(const PeelArgs& a, const Smem& s, int rank, unsigned G,
     n_out += total;
     ok = ks_grid_sync(a.bar, G, epoch, a.err, a.limit_ns);
   }
+  // one read of the error word for the whole block
+  const int e = __syncthreads_or(tid == 0 && ks_ld_volatile(a.err) != 0) ? ks_ld_volatile(a.err) : 0;
   if (rank == 0 && tid == 0) {
-    const int e = ks_ld_volatile(a.err);
     a.info[0] = n_out;
     a.info[1] = e ? e : status;
     a.info[2] = it;
     if (status != KS_ERR_OVERFLOW) a.info[3] = n_out;
   }
+  return PeelOutcome{n_out, it, e ? e : status};
 }
 
 __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   const Smem s = carve_smem(a, smem_raw);
   unsigned epoch = 0;
-  run_peel(a, s, blockIdx.x, gridDim.x, epoch);
+  run_peel<kRowsPerWarp>(a, s, blockIdx.x, gridDim.x, epoch);
 }
 
 struct ResSmem {
-  const float* W;  // P*nt
+  const float* W;  // Wt[t][8]: the basis transposed, components padded to 8
   int* xl_tau;     // warps*kXList
   int* xl_k;
   float* xl_amp;
@@ -785,19 +811,23 @@ __device__ void residual_item(const PeelArgs& a, const ResSmem& s, int n_iter, l
       const int tau = s.xl_tau[warp * kXList + e];
       const int k = s.xl_k[warp * kXList + e];
       const float amp = s.xl_amp[warp * kXList + e];
+      const int t0 = c0 - tau + half;   // tap of column c0
       float u[8];
 #pragma unroll
       for (int pp = 0; pp < 8; ++pp)
         u[pp] = (chok && pp < P) ? __ldg(a.U + ((long long)k * P + pp) * a.C + c) : 0.f;
-      const int t0 = c0 - tau + half;   // tap of column c0
+      const float4* W4 = reinterpret_cast<const float4*>(s.W);
 #pragma unroll
       for (int j = 0; j < kCol; ++j) {
         const int t = t0 + j;
         if (t >= 0 && t < nt) {
+          // the tap's P components: two broadcast 16-byte loads
+          const float4 wa = W4[2 * t], wb = W4[2 * t + 1];
+          const float wt[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
           float wv = 0.f;
 #pragma unroll
           for (int pp = 0; pp < 8; ++pp)
-            if (pp < P) wv = fmaf(u[pp], s.W[pp * nt + t], wv);
+            if (pp < P) wv = fmaf(u[pp], wt[pp], wv);
           x[j] = __fsub_rn(x[j], __fmul_rn(amp, wv));
         }
       }
@@ -817,13 +847,12 @@ __global__ void __launch_bounds__(kResThreads)
 ks_residual_kernel(PeelArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   float* sW = reinterpret_cast<float*>(smem_raw);
-  const int wn = (a.P * a.nt + 3) & ~3;
   ResSmem s;
   s.W = sW;
-  s.xl_tau = reinterpret_cast<int*>(sW + wn);
+  s.xl_tau = reinterpret_cast<int*>(sW + 8 * a.nt);
   s.xl_k = s.xl_tau + kResWarps * kXList;
   s.xl_amp = reinterpret_cast<float*>(s.xl_k + kResWarps * kXList);
-  for (int i = threadIdx.x; i < a.P * a.nt; i += kResThreads) sW[i] = a.W[i];
+  stage_basis_t8(a.W, a.P, a.nt, sW, kResThreads);
   __syncthreads();
   const long long n_out = a.info[0];
   const int status = (int)a.info[1];
@@ -838,7 +867,8 @@ ks_residual_kernel(PeelArgs a) {
 }
 
 size_t residual_smem_bytes(int P, int nt) {
-  return sizeof(float) * (((size_t)P * nt + 3) & ~size_t(3)) +
+  (void)P;
+  return sizeof(float) * 8 * (size_t)nt +
          (size_t)kResWarps * kXList * (2 * sizeof(int) + sizeof(float));
 }
 

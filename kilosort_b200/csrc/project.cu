@@ -70,51 +70,76 @@ constexpr int kTT = 128;   // samples per tile
 constexpr int kCG = 16;    // channels per tile
 constexpr int kPMax = 8;
 
+// X window per channel: samples tau0 - nt/2 .. tau0 + kTT + nt + 7, padded so
+// every row starts on a 16-byte boundary.
+__host__ __device__ inline int temporal_xw(int nt) { return (kTT + nt + 8 + 3) & ~3; }
+
+// Each thread owns 8 consecutive samples of one channel and all PP components.
+// Taps run in groups of 8 over a 16-sample register window, so every operand
+// index is a compile-time constant (no register shifting); the tap's components
+// come from the transposed basis Wt[t][8] as two broadcast 16-byte loads.
+// acc[i][p] accumulates taps t = 0 .. nt-1 in increasing order.
 template <int PP>
 __global__ void __launch_bounds__(256)
 ks_temporal_kernel(const float* __restrict__ X, const float* __restrict__ W,
                    int C, int L, int nt, int Q, float* __restrict__ Yf,
                    __nv_bfloat16* __restrict__ Yhi, __nv_bfloat16* __restrict__ Ylo) {
   extern __shared__ __align__(16) float sm[];
-  const int xw = kTT + nt + 7;              // X window per channel (+ slack)
+  const int xw = temporal_xw(nt);
+  const int ntr = (nt + 7) & ~7;            // taps rounded to the group of 8
   float* sX = sm;                           // [kCG][xw]
-  float* sW = sX + kCG * xw;                // [nt][PP]  (tap-major)
-  float* sY = sW + ((nt * PP + 3) & ~3);    // [kTT][kCG*PP]
+  float* sW = sX + kCG * xw;                // Wt[ntr][8] (zero past nt and P)
+  float* sY = sW + 8 * ntr;                 // [kTT][kCG*PP]
   const int tau0 = blockIdx.x * kTT;
   const int cg0 = blockIdx.y * kCG;
   const int half = nt / 2;
-  for (int i = threadIdx.x; i < kCG * xw; i += 256) {
-    const int cl = i / xw, u = i - cl * xw;
-    const int c = cg0 + cl, t = tau0 - half + u;
-    sX[i] = (c < C && t >= 0 && t < L) ? X[(long long)c * L + t] : 0.f;
+  for (int cl = 0; cl < kCG; ++cl) {
+    const int c = cg0 + cl;
+    const float* xrow = X + (long long)(c < C ? c : 0) * L;
+    for (int u = threadIdx.x; u < xw; u += 256) {
+      const int t = tau0 - half + u;
+      sX[cl * xw + u] = (c < C && t >= 0 && t < L) ? xrow[t] : 0.f;
+    }
   }
-  for (int i = threadIdx.x; i < nt * PP; i += 256) {
-    const int t = i / PP, p = i - t * PP;
-    sW[i] = W[p * nt + t];
+  for (int i = threadIdx.x; i < 8 * ntr; i += 256) {
+    const int t = i >> 3, p = i & 7;
+    sW[i] = (p < PP && t < nt) ? W[p * nt + t] : 0.f;
   }
   __syncthreads();
   const int cl = threadIdx.x & (kCG - 1);
   const int g = threadIdx.x / kCG;          // 16 groups of 8 samples
-  const float* xs = sX + cl * xw + g * 8;
+  const float4* xs4 = reinterpret_cast<const float4*>(sX + cl * xw + g * 8);
+  const float4* w4 = reinterpret_cast<const float4*>(sW);
   float acc[8][PP];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int p = 0; p < PP; ++p) acc[i][p] = 0.f;
-  float win[8];
+  float win[16];
+  {
+    const float4 a = xs4[0], b = xs4[1];
+    win[0] = a.x; win[1] = a.y; win[2] = a.z; win[3] = a.w;
+    win[4] = b.x; win[5] = b.y; win[6] = b.z; win[7] = b.w;
+  }
+  for (int t0 = 0; t0 < nt; t0 += 8) {
+    {
+      const float4 a = xs4[(t0 >> 2) + 2], b = xs4[(t0 >> 2) + 3];
+      win[8] = a.x; win[9] = a.y; win[10] = a.z; win[11] = a.w;
+      win[12] = b.x; win[13] = b.y; win[14] = b.z; win[15] = b.w;
+    }
 #pragma unroll
-  for (int i = 0; i < 8; ++i) win[i] = xs[i];
-  for (int t = 0; t < nt; ++t) {
-    float w[PP];
+    for (int tt = 0; tt < 8; ++tt) {
+      if (t0 + tt < nt) {
+        const float4 wa = w4[2 * (t0 + tt)], wb = w4[2 * (t0 + tt) + 1];
+        const float w[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
 #pragma unroll
-    for (int p = 0; p < PP; ++p) w[p] = sW[t * PP + p];
+        for (int i = 0; i < 8; ++i)
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+          for (int p = 0; p < PP; ++p) acc[i][p] = fmaf(w[p], win[i + tt], acc[i][p]);
+      }
+    }
 #pragma unroll
-      for (int p = 0; p < PP; ++p) acc[i][p] = fmaf(w[p], win[i], acc[i][p]);
-#pragma unroll
-    for (int i = 0; i < 7; ++i) win[i] = win[i + 1];
-    win[7] = xs[t + 8];
+    for (int i = 0; i < 8; ++i) win[i] = win[i + 8];
   }
   const int row = kCG * PP;
 #pragma unroll
@@ -122,23 +147,37 @@ ks_temporal_kernel(const float* __restrict__ X, const float* __restrict__ W,
 #pragma unroll
     for (int p = 0; p < PP; ++p) sY[(g * 8 + i) * row + cl * PP + p] = acc[i][p];
   __syncthreads();
+  // rows of kCG*PP values (a multiple of 8) leave in 8-value pieces: 32-byte
+  // (f32) or 16-byte (bf16 hi and lo) stores, Q and q0 being multiples of 8
   const long long q0 = (long long)cg0 * PP;
-  for (int e = threadIdx.x; e < kTT * row; e += 256) {
-    const int r = e / row, q = e - r * row;
+  constexpr int kPieces = kCG * PP / 8;
+  for (int e = threadIdx.x; e < kTT * kPieces; e += 256) {
+    const int r = e / kPieces, q = (e - r * kPieces) * 8;
+    const float4 va = *reinterpret_cast<const float4*>(sY + r * row + q);
+    const float4 vb = *reinterpret_cast<const float4*>(sY + r * row + q + 4);
     const long long o = (long long)(tau0 + r) * Q + q0 + q;
-    const float v = sY[e];
-    if (Yf) Yf[o] = v;
+    if (Yf) {
+      reinterpret_cast<float4*>(Yf + o)[0] = va;
+      reinterpret_cast<float4*>(Yf + o)[1] = vb;
+    }
     if (Yhi) {
-      const __nv_bfloat16 h = __float2bfloat16_rn(v);
-      Yhi[o] = h;
-      Ylo[o] = __float2bfloat16_rn(v - __bfloat162float(h));
+      const float v[8] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
+      __nv_bfloat162 hi[4], lo[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        hi[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+        const float2 hf = __bfloat1622float2(hi[j]);
+        lo[j] = __floats2bfloat162_rn(v[2 * j] - hf.x, v[2 * j + 1] - hf.y);
+      }
+      *reinterpret_cast<uint4*>(Yhi + o) = *reinterpret_cast<const uint4*>(hi);
+      *reinterpret_cast<uint4*>(Ylo + o) = *reinterpret_cast<const uint4*>(lo);
     }
   }
 }
 
 size_t temporal_smem(int nt, int P) {
-  const int xw = kTT + nt + 7;
-  return sizeof(float) * ((size_t)kCG * xw + ((nt * P + 3) & ~3) + (size_t)kTT * kCG * P);
+  const int ntr = (nt + 7) & ~7;
+  return sizeof(float) * ((size_t)kCG * temporal_xw(nt) + 8 * (size_t)ntr + (size_t)kTT * kCG * P);
 }
 
 // ------------------------------------------------------------------ FP32 GEMM

@@ -118,5 +118,5 @@ def test_batched_workspace_query_and_argument_checks():
     bats[1].rec = 1
     assert lib.ks_match_batches_workspace_size(recs, 2, bats, 300, _lib.KS_PROJ_BF16X3, 2) == 0
     assert lib.ks_match_batches_workspace_size(recs, 2, bats, 3, 7, 2) == 0
-    rc = lib.ks_match_batches(recs, 2, bats, 3, _lib.KS_PROJ_BF16X3, 2, None, 0, None)
+    rc = lib.ks_match_batches(recs, 2, bats, 3, _lib.KS_PROJ_BF16X3, 2, 1, None, 0, None, None)
     assert rc == _lib.KS_ERR_WORKSPACE

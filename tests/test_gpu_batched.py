@@ -65,14 +65,15 @@ def _reference(setup, items, projection):
 
 
 @pytest.mark.parametrize("projection", ["fp32", "bf16x3"])
-@pytest.mark.parametrize("teams", [0, 1, 3, 8])
-def test_batched_equals_per_batch(cuda_device, projection, teams):
+@pytest.mark.parametrize("teams,groups", [(0, 1), (1, 1), (3, 1), (8, 1), (2, 3), (8, 2)])
+def test_batched_equals_per_batch(cuda_device, projection, teams, groups):
     recs = _recordings()
     setup = _setup(recs)
     items = _items(recs)
     ref = _reference(setup, items, projection)
     assert sum(len(r[0]) for r in ref) > 100
-    res = match_batches([s[3] for s in setup], items, projection=projection, teams=teams)
+    res = match_batches([s[3] for s in setup], items, projection=projection, teams=teams,
+                        groups=groups)
     _assert_same(res, ref)
 
 
@@ -102,14 +103,14 @@ def test_overflowing_batch_reports_and_others_complete(cuda_device):
         m.results()
 
 
-@pytest.mark.parametrize("projection", ["fp32", "bf16x3"])
-def test_graph_replay_with_new_inputs(cuda_device, projection):
+@pytest.mark.parametrize("projection,groups", [("fp32", 1), ("bf16x3", 1), ("bf16x3", 3)])
+def test_graph_replay_with_new_inputs(cuda_device, projection, groups):
     recs = _recordings()
     setup = _setup(recs)
     items = _items(recs)
     ref = _reference(setup, items, projection)
     m = BatchedMatcher([s[3] for s in setup], [(X.shape[1], r) for X, r in items],
-                       projection, teams=4, graph=True)
+                       projection, teams=4, graph=True, groups=groups)
     # first replay on zeros-scaled inputs, then on the real ones: the graph
     # reads the buffers, not values captured at capture time
     # results are views of the matcher's buffers: keep copies across runs
