@@ -442,11 +442,13 @@ __device__ __forceinline__ TouchList load_touch_warp(const PeelArgs& a, const Sm
 // columns are touched by one peak; its cross-correlations are loaded with the
 // rows of B (16 rows per round trip).  Later peaks of the same column (at
 // most one more unless scores tie exactly) are applied in a second round, in
-// the same order.
+// the same order.  A column no peak touches keeps its rows, so its score is
+// its settled one (cfmax/imax): the item holding row 0 passes that on instead
+// of re-reading the rows (all columns are scored from B when init is set).
 template <int kRows>
 __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk,
                                  int j_lo, int j_hi, unsigned long long* pack_out,
-                                 int lane) {
+                                 int lane, bool init = false) {
   const int c = blk * kCol + lane;
   const bool colok = c < a.L;
   const int nt = a.nt, K = a.K, nlag = 2 * nt + 1;
@@ -460,6 +462,7 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
     }
   }
   const bool touched = e0 >= 0;
+  const bool score = init || touched;
   const bool any_rest = __any_sync(0xffffffffu, rest != 0u);
   const float* cp0 = a.ctcT;
   float amp0 = 0.f;
@@ -472,7 +475,7 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
 #pragma unroll
     for (int r = 0; r < kRows; ++r) {
       const int j = j0 + r;
-      const bool ok = colok && j < j_hi;
+      const bool ok = score && colok && j < j_hi;
       bv[r] = ok ? bcol[(size_t)j * kCol] : 0.f;
       w0[r] = (ok && e0 >= 0) ? __ldg(cp0 + (size_t)j * nlag) : 0.f;
     }
@@ -498,13 +501,19 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
 #pragma unroll
     for (int r = 0; r < kRows; ++r) {
       const int j = j0 + r;
-      if (colok && j < j_hi) {
+      if (score && colok && j < j_hi) {
         if (touched) bcol[(size_t)j * kCol] = bv[r];
         fold_score(bv[r], __ldg(a.nmi + j), j, best, arg);
       }
     }
   }
-  if (colok && best >= 0.f) atomicMax(&pack_out[c], pack_score(best, arg));
+  if (colok) {
+    if (score) {
+      if (best >= 0.f) atomicMax(&pack_out[c], pack_score(best, arg));
+    } else if (j_lo == 0) {
+      atomicMax(&pack_out[c], pack_score(a.cfmax[c], a.imax[c]));
+    }
+  }
 }
 
 // Block of the rank-th set bit of the dirty bitmap (s.wprefix holds the
@@ -578,7 +587,8 @@ __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsi
     const long long n_items = (long long)a.nblk * rg;
     for (long long w = gwarp; w < n_items; w += nwarps) {
       const int blk = (int)(w / rg), r = (int)(w % rg);
-      update_warp_item<kRows>(a, none, blk, r * kItemRows, min(a.K, (r + 1) * kItemRows), pinit, lane);
+      update_warp_item<kRows>(a, none, blk, r * kItemRows, min(a.K, (r + 1) * kItemRows), pinit,
+                              lane, true);
     }
   }
 
@@ -604,9 +614,10 @@ __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsi
       if (rank == 0 && tid == 0) a.info[3] = n_out + total;
       break;
     }
-    for (int ch = rank; ch < a.nchunks; ch += (int)G) {
+    // one warp per chunk (the chunks' peak counts are independent loads)
+    for (int ch = rank * kWarps + warp; ch < a.nchunks; ch += (int)G * kWarps) {
       const int c_n = a.chunk_cnt[ch];
-      for (int i = tid; i < c_n; i += kThreads) {
+      for (int i = lane; i < c_n; i += 32) {
         const long long slot = (long long)ch * kChunk + i;
         const long long o = n_out + s.prefix[ch] + i;
         const int tau = a.chunk_tau[slot];

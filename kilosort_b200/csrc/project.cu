@@ -68,116 +68,156 @@ __global__ void ks_reorder_templates_kernel(const float* __restrict__ U, int K,
 // ------------------------------------------------------------------ temporal
 constexpr int kTT = 128;   // samples per tile
 constexpr int kCG = 16;    // channels per tile
+constexpr int kTemporalThreads = 256;
 constexpr int kPMax = 8;
 
 // X window per channel: samples tau0 - nt/2 .. tau0 + kTT + nt + 7, padded so
 // every row starts on a 16-byte boundary.
 __host__ __device__ inline int temporal_xw(int nt) { return (kTT + nt + 8 + 3) & ~3; }
 
-// Each thread owns 8 consecutive samples of one channel and all PP components.
-// Taps run in groups of 8 over a 16-sample register window, so every operand
-// index is a compile-time constant (no register shifting); the tap's components
-// come from the transposed basis Wt[t][8] as two broadcast 16-byte loads.
-// acc[i][p] accumulates taps t = 0 .. nt-1 in increasing order.
+// Asynchronous 4-byte global -> shared copy; src_bytes 0 fills zeros.
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, int src_bytes) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+
+// Persistent: block b takes tiles b, b + grid, ... (a tile is kTT samples x
+// kCG channels).  The X window of the next tile is copied (cp.async) while the
+// current one is computed.  Each thread owns 8 consecutive samples of one
+// channel and all PP components; taps run in groups of 8 over a 16-sample
+// register window (every operand index a compile-time constant) and each
+// tap's components come from the transposed basis Wt[t][8] as two broadcast
+// 16-byte loads.  acc[i][p] accumulates taps t = 0 .. nt-1 in increasing
+// order.  Results go straight from registers to Y: the PP values of one
+// (sample, channel) are contiguous there.
 template <int PP>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kTemporalThreads)
 ks_temporal_kernel(const float* __restrict__ X, const float* __restrict__ W,
-                   int C, int L, int nt, int Q, float* __restrict__ Yf,
-                   __nv_bfloat16* __restrict__ Yhi, __nv_bfloat16* __restrict__ Ylo) {
+                   int C, int L, int nt, int Q, int tiles_t, int n_tiles,
+                   float* __restrict__ Yf, __nv_bfloat16* __restrict__ Yhi,
+                   __nv_bfloat16* __restrict__ Ylo) {
   extern __shared__ __align__(16) float sm[];
+  constexpr int kS = kTT / (kTemporalThreads / kCG);   // samples per thread (8)
   const int xw = temporal_xw(nt);
   const int ntr = (nt + 7) & ~7;            // taps rounded to the group of 8
-  float* sX = sm;                           // [kCG][xw]
-  float* sW = sX + kCG * xw;                // Wt[ntr][8] (zero past nt and P)
-  float* sY = sW + 8 * ntr;                 // [kTT][kCG*PP]
-  const int tau0 = blockIdx.x * kTT;
-  const int cg0 = blockIdx.y * kCG;
+  float* sW = sm;                           // Wt[ntr][8] (zero past nt and PP)
+  float* sX[2] = {sW + 8 * ntr, sW + 8 * ntr + kCG * xw};   // [kCG][xw] each
   const int half = nt / 2;
-  for (int cl = 0; cl < kCG; ++cl) {
-    const int c = cg0 + cl;
-    const float* xrow = X + (long long)(c < C ? c : 0) * L;
-    for (int u = threadIdx.x; u < xw; u += 256) {
-      const int t = tau0 - half + u;
-      sX[cl * xw + u] = (c < C && t >= 0 && t < L) ? xrow[t] : 0.f;
-    }
-  }
-  for (int i = threadIdx.x; i < 8 * ntr; i += 256) {
+  for (int i = threadIdx.x; i < 8 * ntr; i += kTemporalThreads) {
     const int t = i >> 3, p = i & 7;
     sW[i] = (p < PP && t < nt) ? W[p * nt + t] : 0.f;
   }
-  __syncthreads();
+  auto fetch = [&](int tile, float* dst) {
+    const int tau0 = (tile % tiles_t) * kTT, cg0 = (tile / tiles_t) * kCG;
+    for (int cl = 0; cl < kCG; ++cl) {
+      const int c = cg0 + cl;
+      const float* xrow = X + (long long)(c < C ? c : 0) * L;
+      for (int u = threadIdx.x; u < xw; u += kTemporalThreads) {
+        const int t = tau0 - half + u;
+        const bool ok = c < C && t >= 0 && t < L;
+        cp_async4(dst + cl * xw + u, ok ? xrow + t : X, ok ? 4 : 0);
+      }
+    }
+    cp_async_commit();
+  };
   const int cl = threadIdx.x & (kCG - 1);
-  const int g = threadIdx.x / kCG;          // 16 groups of 8 samples
-  const float4* xs4 = reinterpret_cast<const float4*>(sX + cl * xw + g * 8);
-  const float4* w4 = reinterpret_cast<const float4*>(sW);
-  float acc[8][PP];
+  const int g = threadIdx.x / kCG;          // groups of kS samples
+  int buf = 0;
+  if (blockIdx.x < n_tiles) fetch(blockIdx.x, sX[0]);
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int next = tile + gridDim.x;
+    if (next < n_tiles) fetch(next, sX[buf ^ 1]);
+    else cp_async_commit();                 // keep the group count in step
+    cp_async_wait_prev();                   // this tile's window has landed
+    __syncthreads();
+    const int tau0 = (tile % tiles_t) * kTT, cg0 = (tile / tiles_t) * kCG;
+    const float4* xs4 = reinterpret_cast<const float4*>(sX[buf] + cl * xw + g * kS);
+    float acc[kS][PP];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < kS; ++i)
 #pragma unroll
-    for (int p = 0; p < PP; ++p) acc[i][p] = 0.f;
-  float win[16];
-  {
-    const float4 a = xs4[0], b = xs4[1];
-    win[0] = a.x; win[1] = a.y; win[2] = a.z; win[3] = a.w;
-    win[4] = b.x; win[5] = b.y; win[6] = b.z; win[7] = b.w;
-  }
-  for (int t0 = 0; t0 < nt; t0 += 8) {
-    {
-      const float4 a = xs4[(t0 >> 2) + 2], b = xs4[(t0 >> 2) + 3];
-      win[8] = a.x; win[9] = a.y; win[10] = a.z; win[11] = a.w;
-      win[12] = b.x; win[13] = b.y; win[14] = b.z; win[15] = b.w;
+      for (int p = 0; p < PP; ++p) acc[i][p] = 0.f;
+    float win[kS + 8];
+#pragma unroll
+    for (int k = 0; k < kS / 4; ++k) {
+      const float4 a = xs4[k];
+      win[4 * k] = a.x; win[4 * k + 1] = a.y; win[4 * k + 2] = a.z; win[4 * k + 3] = a.w;
     }
+    const float4* w4 = reinterpret_cast<const float4*>(sW);
+    for (int t0 = 0; t0 < nt; t0 += 8) {
+      {
+        const float4 a = xs4[(t0 + kS) / 4], b = xs4[(t0 + kS) / 4 + 1];
+        win[kS + 0] = a.x; win[kS + 1] = a.y; win[kS + 2] = a.z; win[kS + 3] = a.w;
+        win[kS + 4] = b.x; win[kS + 5] = b.y; win[kS + 6] = b.z; win[kS + 7] = b.w;
+      }
 #pragma unroll
-    for (int tt = 0; tt < 8; ++tt) {
-      if (t0 + tt < nt) {
-        const float4 wa = w4[2 * (t0 + tt)], wb = w4[2 * (t0 + tt) + 1];
-        const float w[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+      for (int tt = 0; tt < 8; ++tt) {
+        if (t0 + tt < nt) {
+          const float4 wa = w4[2 * (t0 + tt)], wb = w4[2 * (t0 + tt) + 1];
+          const float w[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+          for (int i = 0; i < kS; ++i)
 #pragma unroll
-          for (int p = 0; p < PP; ++p) acc[i][p] = fmaf(w[p], win[i + tt], acc[i][p]);
+            for (int p = 0; p < PP; ++p) acc[i][p] = fmaf(w[p], win[i + tt], acc[i][p]);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < kS; ++i) win[i] = win[i + 8];
+    }
+    // the window is no longer read: the next fetch may overwrite this buffer
+    __syncthreads();
+    const long long q0 = (long long)(cg0 + cl) * PP;
+#pragma unroll
+    for (int i = 0; i < kS; ++i) {
+      const long long o = (long long)(tau0 + g * kS + i) * Q + q0;
+      // pairs of components as one 8-byte (f32) or 4-byte (bf16) store: with
+      // PP even, o + p is even for even p
+      if (Yf) {
+#pragma unroll
+        for (int p = 0; p < PP; p += 2) {
+          if (PP % 2 == 0)
+            *reinterpret_cast<float2*>(Yf + o + p) = make_float2(acc[i][p], acc[i][p + 1]);
+          else {
+            Yf[o + p] = acc[i][p];
+            if (p + 1 < PP) Yf[o + p + 1] = acc[i][p + 1];
+          }
+        }
+      }
+      if (Yhi) {
+#pragma unroll
+        for (int p = 0; p < PP; p += 2) {
+          const float v0 = acc[i][p], v1 = p + 1 < PP ? acc[i][p + 1] : 0.f;
+          const __nv_bfloat162 h = __floats2bfloat162_rn(v0, v1);
+          const float2 hf = __bfloat1622float2(h);
+          const __nv_bfloat162 l = __floats2bfloat162_rn(v0 - hf.x, v1 - hf.y);
+          if (PP % 2 == 0) {
+            *reinterpret_cast<__nv_bfloat162*>(Yhi + o + p) = h;
+            *reinterpret_cast<__nv_bfloat162*>(Ylo + o + p) = l;
+          } else {
+            Yhi[o + p] = h.x;
+            Ylo[o + p] = l.x;
+            if (p + 1 < PP) {
+              Yhi[o + p + 1] = h.y;
+              Ylo[o + p + 1] = l.y;
+            }
+          }
+        }
       }
     }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) win[i] = win[i + 8];
+    buf ^= 1;
   }
-  const int row = kCG * PP;
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int p = 0; p < PP; ++p) sY[(g * 8 + i) * row + cl * PP + p] = acc[i][p];
-  __syncthreads();
-  // rows of kCG*PP values (a multiple of 8) leave in 8-value pieces: 32-byte
-  // (f32) or 16-byte (bf16 hi and lo) stores, Q and q0 being multiples of 8
-  const long long q0 = (long long)cg0 * PP;
-  constexpr int kPieces = kCG * PP / 8;
-  for (int e = threadIdx.x; e < kTT * kPieces; e += 256) {
-    const int r = e / kPieces, q = (e - r * kPieces) * 8;
-    const float4 va = *reinterpret_cast<const float4*>(sY + r * row + q);
-    const float4 vb = *reinterpret_cast<const float4*>(sY + r * row + q + 4);
-    const long long o = (long long)(tau0 + r) * Q + q0 + q;
-    if (Yf) {
-      reinterpret_cast<float4*>(Yf + o)[0] = va;
-      reinterpret_cast<float4*>(Yf + o)[1] = vb;
-    }
-    if (Yhi) {
-      const float v[8] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
-      __nv_bfloat162 hi[4], lo[4];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        hi[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
-        const float2 hf = __bfloat1622float2(hi[j]);
-        lo[j] = __floats2bfloat162_rn(v[2 * j] - hf.x, v[2 * j + 1] - hf.y);
-      }
-      *reinterpret_cast<uint4*>(Yhi + o) = *reinterpret_cast<const uint4*>(hi);
-      *reinterpret_cast<uint4*>(Ylo + o) = *reinterpret_cast<const uint4*>(lo);
-    }
-  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 size_t temporal_smem(int nt, int P) {
+  (void)P;
   const int ntr = (nt + 7) & ~7;
-  return sizeof(float) * ((size_t)kCG * temporal_xw(nt) + 8 * (size_t)ntr + (size_t)kTT * kCG * P);
+  return sizeof(float) * (8 * (size_t)ntr + 2 * (size_t)kCG * temporal_xw(nt));
 }
 
 // ------------------------------------------------------------------ FP32 GEMM
@@ -341,13 +381,26 @@ int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
                     int64_t P, int64_t nt, int64_t Q, int64_t Lpad, float* Yf,
                     __nv_bfloat16* Yhi, __nv_bfloat16* Ylo, cudaStream_t stream) {
   const size_t smem = temporal_smem((int)nt, (int)P);
-  dim3 grid((unsigned)(Lpad / kTT), (unsigned)((C + kCG - 1) / kCG));
+  const int tiles_t = (int)(Lpad / kTT);
+  const long long n_tiles = (long long)tiles_t * ((C + kCG - 1) / kCG);
+  if (n_tiles > 0x7fffffffLL) return fail(KS_ERR_UNSUPPORTED, "project: too many temporal tiles");
+  DeviceInfo dev;
+  int drc = device_info(&dev);
+  if (drc) return drc;
+  // persistent: as many blocks as are resident at once
+  int occ = 0;
 #define KS_TEMPORAL_CASE(PPV)                                                              \
   case PPV: {                                                                              \
     KS_CUDA(cudaFuncSetAttribute(ks_temporal_kernel<PPV>,                                  \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-    ks_temporal_kernel<PPV><<<grid, 256, smem, stream>>>(X, W, (int)C, (int)L, (int)nt,    \
-                                                         (int)Q, Yf, Yhi, Ylo);            \
+    KS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ks_temporal_kernel<PPV>,   \
+                                                          kTemporalThreads, smem));        \
+    const unsigned grid =                                                                  \
+        (unsigned)std::min<long long>(n_tiles, (long long)std::max(occ, 1) * dev.sm_count); \
+    ks_temporal_kernel<PPV><<<grid, kTemporalThreads, smem, stream>>>(                     \
+        X, W, (int)C, (int)L, (int)nt,                                                     \
+                                                         (int)Q, tiles_t, (int)n_tiles,    \
+                                                         Yf, Yhi, Ylo);                    \
     break;                                                                                 \
   }
   switch (P) {
