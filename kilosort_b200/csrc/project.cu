@@ -417,7 +417,12 @@ int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
   }
 #undef KS_TEMPORAL_CASE
   KS_CUDA(cudaGetLastError());
-  // q columns past the last channel group are padding: zero them
+  return zero_q_padding(C, P, Q, Lpad, Yf, Yhi, Ylo, stream);
+}
+
+// q columns past the last group of 16 channels are padding: zero them.
+int zero_q_padding(int64_t C, int64_t P, int64_t Q, int64_t Lpad, float* Yf, __nv_bfloat16* Yhi,
+                   __nv_bfloat16* Ylo, cudaStream_t stream) {
   const int64_t qused = round_up(C, kCG) * P;
   if (qused < Q) {
     if (Yf) KS_CUDA(cudaMemset2DAsync(Yf + qused, Q * sizeof(float), 0, (Q - qused) * sizeof(float), Lpad, stream));
@@ -428,6 +433,7 @@ int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
   }
   return KS_OK;
 }
+
 
 int launch_project(const float* X, const float* U, const float* W, int64_t C,
                    int64_t L, int64_t K, int64_t P, int64_t nt, int precision,

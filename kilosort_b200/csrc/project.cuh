@@ -37,6 +37,8 @@ int launch_reorder_templates(const float* U, int64_t K, int64_t P, int64_t C, in
 int launch_temporal(const float* X, const float* W, int64_t C, int64_t L, int64_t P,
                     int64_t nt, int64_t Q, int64_t Lpad, float* Yf, __nv_bfloat16* Yhi,
                     __nv_bfloat16* Ylo, cudaStream_t stream);
+int zero_q_padding(int64_t C, int64_t P, int64_t Q, int64_t Lpad, float* Yf, __nv_bfloat16* Yhi,
+                   __nv_bfloat16* Ylo, cudaStream_t stream);
 // B is written row-major [K, ldb] or, when tiled, in 32-column blocks
 // [ceil(L/32)][K][32] (the layout of the peel).
 // The first 256 bytes of the workspace hold the device error word of the
