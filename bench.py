@@ -43,7 +43,7 @@ TH = 8.0
 CFG = 2
 # DRAM bytes (read + write) of one peel_kernel launch on a C=384/K=600/60000-sample
 # batch, from the ncu capture summarised in profiles/peel_kernel_c384_k600.txt
-PEEL_TRAFFIC_BYTES = 8.709e9
+PEEL_TRAFFIC_BYTES = 8.678e9
 WORKLOAD = ("Neuropixels-scale matching: C=384 (NP1-like), K=600 templates, 20 batches x "
             "60000 samples (+2*61 pad), nt=61, n_pcs=6, Th_learned=8, max_peels=100")
 
