@@ -267,6 +267,23 @@ KS_API int ks_recon_adjoint(const float* Xres, const int64_t* st, const float* a
                             void* stream);
 
 /*
+ * Output consumers of extract: per spike s (template templ[s], features
+ * tF [N, nC, P] as extract returns them), the position estimate
+ *   w_i = m_i ||tF[s,i,:]|| / sum_j m_j ||tF[s,j,:]||, m_i = iCC_mask[i, iU[k]]
+ *   xs[s] = sum_i xc[iCC[i, iU[k]]] w_i,  ys[s] likewise  (double)
+ * and the amplitude amps[s] = ||tF[s,:,:]|| (float).  iCC [nC, C] int64,
+ * iCC_mask [nC, C] uint8, iU [K] int64, xc/yc [C] double.  A template index
+ * outside [0, K) sets *status (device int) to KS_ERR_ARG and gives zeros.
+ * Replaces kilosort/postprocessing.py:33-62 (compute_spike_positions) and the
+ * amplitudes of kilosort/io.py:353.
+ */
+KS_API int ks_spike_positions(const float* tF, const int64_t* templ, const int64_t* iCC,
+                              const uint8_t* iCC_mask, const int64_t* iU, const double* xc,
+                              const double* yc, int64_t N, int64_t nC, int64_t P, int64_t C,
+                              int64_t K, double* xs, double* ys, float* amps, int* status,
+                              void* stream);
+
+/*
  * Stage timing of ks_run_matching, for profiling the public call as it runs
  * (no work is skipped or added).  While enabled on the calling host thread,
  * ks_run_matching records CUDA events at five points on its stream: start,

@@ -1,0 +1,31 @@
+"""CPU oracle of the output consumers of `extract`.
+
+TEST INFRASTRUCTURE ONLY.  Restates with the same PyTorch ops:
+
+* ``spike_positions`` -- kilosort/postprocessing.py:33-62
+  (compute_spike_positions): per spike, the 2-norm of its PC features on each
+  of the nC channels nearest its template's peak channel, masked by
+  ``iCC_mask``, normalised to sum 1, weights the channels' x and y;
+* ``amplitudes`` -- kilosort/io.py:353: the 2-norm of each spike's features.
+
+Pinned against tests/golden/golden_post.npz (the reference's own outputs).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+
+def spike_positions(st, tF, iCC, iCC_mask, iU, xc, yc):
+    tmass = torch.norm(tF, 2, dim=-1)
+    tmask = iCC_mask[:, iU[st[:, 1]]].T
+    tmass = tmass * tmask
+    tmass = tmass / tmass.sum(1, keepdim=True)
+    chs = iCC[:, iU[st[:, 1]]]
+    xc0 = torch.from_numpy(xc)[chs.T]
+    yc0 = torch.from_numpy(yc)[chs.T]
+    return (xc0 * tmass).sum(1).numpy(), (yc0 * tmass).sum(1).numpy()
+
+
+def amplitudes(tF):
+    return torch.norm(tF, dim=[-2, -1]).numpy()

@@ -1,0 +1,58 @@
+"""Golden vectors of the reference's output consumers of `extract`.
+
+Run from the repository root in a container that has the reference checkout,
+after make_golden.py:
+
+    python tests/golden/make_golden_post.py [path/to/reference]
+
+Loads the golden `extract` case (tests/golden/golden_extract.npz, its
+recording regenerated from the stored seed), and runs the reference's
+``postprocessing.compute_spike_positions`` (kilosort/postprocessing.py:33-62)
+and the Phy-export amplitudes ``torch.norm(tF, dim=[-2, -1])``
+(kilosort/io.py:353) on it.  ``kilosort.clustering_qr`` (which needs faiss)
+is replaced by an empty stub: compute_spike_positions does not use it.
+Writes tests/golden/golden_post.npz.
+"""
+import ast
+import os
+import sys
+import types
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from kilosort_b200 import synth  # noqa: E402
+
+
+def load_reference(path):
+    pkg = types.ModuleType("kilosort")
+    pkg.__path__ = [os.path.join(path, "kilosort")]
+    sys.modules["kilosort"] = pkg
+    stub = types.ModuleType("kilosort.clustering_qr")
+    stub.xy_templates = None
+    stub.get_data_cpu = None
+    sys.modules["kilosort.clustering_qr"] = stub
+    from kilosort import postprocessing, template_matching
+    return postprocessing, template_matching
+
+
+if __name__ == "__main__":
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    post, tm = load_reference(ref)
+    g = np.load(os.path.join(HERE, "golden_extract.npz"))
+    rec = synth.make_recording(**ast.literal_eval(str(g["seed_kwargs"])))
+    U = torch.from_numpy(rec.U)
+    iCC, iCC_mask, iU, _ = tm.prepare_extract(rec.xc, rec.yc, U, 10, 100,
+                                              device=torch.device("cpu"))
+    ops = dict(iCC=iCC, iCC_mask=iCC_mask, iU=iU, xc=rec.xc, yc=rec.yc)
+    st = g["st"]
+    tF = torch.from_numpy(g["tF"])
+    xs, ys = post.compute_spike_positions(st, tF, ops)
+    amplitudes = torch.norm(tF, dim=[-2, -1]).cpu().numpy()
+    np.savez_compressed(os.path.join(HERE, "golden_post.npz"), xs=xs, ys=ys,
+                        amplitudes=amplitudes, iCC_mask=iCC_mask.numpy())
+    print(f"post: {len(xs)} spikes")

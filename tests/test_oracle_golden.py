@@ -4,6 +4,7 @@ Golden vectors come from running the reference's `prepare_matching`,
 `run_matching`, `prepare_extract` and `extract` (tests/golden/make_golden.py).
 """
 import ast
+import os
 
 import numpy as np
 import pytest
@@ -78,3 +79,19 @@ def test_extract_features_bit_exact():
     order = np.argsort(st_all[:, 0])
     np.testing.assert_array_equal(st_all[order], g["st"])
     np.testing.assert_array_equal(tF[order].numpy(), g["tF"])
+
+
+def test_output_consumers_bit_exact():
+    """Oracle positions and amplitudes equal the reference's on the golden extract."""
+    from kilosort_b200 import synth
+    from oracle import postprocess as op
+    g = gu.load("extract")
+    post = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_post.npz"))
+    kw = ast.literal_eval(str(g["seed_kwargs"]))
+    rec = synth.make_recording(**kw)
+    iCC, mask, iU, _ = om.prepare_extract(rec.xc, rec.yc, torch.from_numpy(rec.U), 10, 100)
+    np.testing.assert_array_equal(mask.numpy(), post["iCC_mask"])
+    xs, ys = op.spike_positions(g["st"], torch.from_numpy(g["tF"]), iCC, mask, iU, rec.xc, rec.yc)
+    np.testing.assert_array_equal(xs, post["xs"])
+    np.testing.assert_array_equal(ys, post["ys"])
+    np.testing.assert_array_equal(op.amplitudes(torch.from_numpy(g["tF"])), post["amplitudes"])
