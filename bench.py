@@ -56,13 +56,17 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batches", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="np1", choices=["np1", "uneven", "adjoint"],
+    p.add_argument("--workload", default="np1", choices=["np1", "uneven", "adjoint", "stream"],
                    help="np1: C=384/K=600, 20 equal batches (default); uneven: three "
                         "recordings, 200 batches of uneven length, batched launches; "
                         "adjoint: reconstruction loss + hand-written adjoint on one "
-                        "C=384/K=600 batch with the matcher's spikes")
+                        "C=384/K=600 batch with the matcher's spikes; stream: int16 host "
+                        "stream -> whitening -> batched matcher, C=384/K=2000, with "
+                        "periodic template refinement")
     p.add_argument("--group", type=int, default=50,
                    help="uneven workload: batches per batched call (one graph each)")
+    p.add_argument("--group-stream", type=int, default=4,
+                   help="stream workload: batches per batched call")
     return p.parse_args()
 
 
@@ -329,6 +333,80 @@ def adjoint_main(args, dev, rank, world):
     if rank == 0:
         print(json.dumps(line), flush=True)
 
+STREAM = ("long dense recording, shortened: C=384 (NP1-like), K=2000 templates (amplitudes "
+          "5-40 sd, 1-30 Hz), {nb} batches of 60000 samples streamed from page-locked host "
+          "int16 (channel-mixed, scale 200) through GPU whitening into the batched split-BF16 "
+          "matcher, one adjoint template-refinement step per group")
+
+
+def stream_main(args, dev, rank, world):
+    """Config 5 on a shortened recording: host int16 -> results on the host."""
+    import kilosort_b200 as kb  # noqa: F401
+    from kilosort_b200 import synth
+    from kilosort_b200.stream import StreamMatcher
+    nb = args.batches if args.batches != 20 else 8
+    rec = synth.make_recording(1005, n_chan=384, probe="np1", n_templates=2000,
+                               batch_lengths=[NT_BATCH] * nb, rate_hz=(1.0, 30.0),
+                               amp_sd=(5.0, 40.0))
+    C = rec.n_chan
+    rng = np.random.default_rng(1005)
+    M = np.eye(C)
+    for d in (1, 2):
+        v = 0.25 / d * (1 + 0.2 * rng.standard_normal(C - d))
+        M += np.diag(v, d) + np.diag(v, -d)
+    # nb whole batches of the recording (the synthetic signal carries a margin)
+    sig = rec.signal[:, :nb * NT_BATCH].astype(np.float64)
+    raw = np.clip(np.round(200.0 * (M @ sig)).T, -32768, 32767)
+    raw = np.ascontiguousarray(raw.astype(np.int16))
+    Wrot = torch.from_numpy(np.linalg.inv(M)).float()
+    U0 = torch.from_numpy(rec.U).to(dev)
+    W = torch.from_numpy(rec.wPCA).to(dev)
+    ops = dict(Th_learned=TH, nt=NT, max_peels=100, wPCA=W)
+    U = U0.clone()
+    sm = StreamMatcher(raw, Wrot, 1.0 / 200.0, ops, U, NT=NT_BATCH, group=args.group_stream,
+                       teams=None, refine_every=1, refine_lr=1e-7)
+    for _ in range(max(1, args.warmup)):
+        sm.run()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev.index or 0)
+    sampler.__enter__()
+    t0 = time.perf_counter()
+    nsp = 0
+    for _ in range(args.steps):
+        times, templ, amps, _ = sm.run()
+        nsp = len(times)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / args.steps
+    sampler.__exit__()
+    sm.close()
+    samples = C * raw.shape[0]
+    value = samples * world / dt
+    h2d = sum((stop - start) for start, stop, _ in sm.windows) * C * 2
+    line = {
+        "metric": "channel-samples/s", "value": value, "unit": "channel-samples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int16 in, f32 (split-bf16 whitening and projection)", "data": "synthetic",
+        "config": {"workload": STREAM.format(nb=nb), "batches": sm.n_batches,
+                   "group": sm.group, "teams": sm.matchers[0].teams,
+                   "refinements_per_step": sm.refinements // (args.steps + max(1, args.warmup)),
+                   "timing": "host wall clock around the whole stream (host int16 in, "
+                             "spike arrays on the host out)",
+                   "parallelism": f"replicas x{world}"},
+        "spikes_per_step": nsp,
+        "spikes_per_s": nsp * world / dt,
+        # per batch: matrix split, raw split, whitening contraction, temporal
+        # projection; per group: energy, {nm, 1/nm}, reorder, contraction,
+        # peel; per refinement: loss (5), adjoint (6), ctc (3), transpose (1)
+        "gpu_launches": (4 * sm.n_batches + 5 * -(-sm.n_batches // sm.group)
+                         + 15 * (sm.refinements // (args.steps + max(1, args.warmup)))),
+        "e2e": {"value": value, "unit": "channel-samples/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": nsp * 20},
+        "clocks": sampler.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
 
 def main():
     args = parse()
@@ -346,8 +424,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
 
-    if args.workload in ("uneven", "adjoint"):
-        (uneven_main if args.workload == "uneven" else adjoint_main)(args, dev, rank, world)
+    if args.workload in ("uneven", "adjoint", "stream"):
+        {"uneven": uneven_main, "adjoint": adjoint_main,
+         "stream": stream_main}[args.workload](args, dev, rank, world)
         if world > 1:
             dist.destroy_process_group()
         return

@@ -267,6 +267,22 @@ KS_API int ks_recon_adjoint(const float* Xres, const int64_t* st, const float* a
                             void* stream);
 
 /*
+ * Whitening of raw int16 samples (the streaming front end):
+ *   X[c, t] = sum_c' Wrot[c, c'] * scale * raw[t * ld_raw + c']   (t < T, c < C)
+ * with raw in the recording's layout (samples x channels), X row-major
+ * [C, ldx].  Split-BF16 on the tensor cores: int16 values are exact as bf16
+ * hi + lo, the matrix (scale folded in) is split as in the score
+ * contraction.  status (device int) receives KS_OK or the contraction's
+ * device error.  Replaces the whitening step of kilosort/io.py:1019-1025
+ * (X = whiten_mat @ X) for raw batches.
+ */
+KS_API size_t ks_whiten_int16_workspace_size(int64_t T, int64_t C);
+KS_API int ks_whiten_int16(const int16_t* raw, int64_t T, int64_t C, int64_t ld_raw,
+                           const float* Wrot, float scale, float* X, int64_t ldx,
+                           int* status, void* workspace, size_t workspace_bytes,
+                           void* stream);
+
+/*
  * Output consumers of extract: per spike s (template templ[s], features
  * tF [N, nC, P] as extract returns them), the position estimate
  *   w_i = m_i ||tF[s,i,:]|| / sum_j m_j ||tF[s,j,:]||, m_i = iCC_mask[i, iU[k]]

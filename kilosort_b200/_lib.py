@@ -66,6 +66,9 @@ SIGNATURES = {
     "ks_recon_adjoint": (_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
                                 _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "ks_spike_positions": (_int, [_vp] * 7 + [_i64] * 5 + [_vp] * 5),
+    "ks_whiten_int16_workspace_size": (_sz, [_i64, _i64]),
+    "ks_whiten_int16": (_int, [_vp, _i64, _i64, _i64, _vp, _f32, _vp, _i64, _vp, _vp, _sz,
+                               _vp]),
     "ks_trace_stages": (_int, [_int]),
     "ks_trace_read": (_int, [_vp, _int]),
     "ks_match_batches_workspace_size": (_sz, [_vp, _i64, _vp, _i64, _int, _i64]),
