@@ -447,11 +447,13 @@ extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
       if (precision == KS_PROJ_BF16X3) {
         __nv_bfloat16* yhi = reinterpret_cast<__nv_bfloat16*>(base + rp.yhi) + (size_t)bp.row_off * rp.Q;
         __nv_bfloat16* ylo = reinterpret_cast<__nv_bfloat16*>(base + rp.ylo) + (size_t)bp.row_off * rp.Q;
-        if ((rc = launch_temporal(d.X, r.W, r.C, d.L, r.P, r.nt, rp.Q, bp.Lpad, nullptr, yhi, ylo, ps)))
+        if ((rc = launch_temporal(d.X, r.W, r.C, d.L, r.P, r.nt, rp.Q, bp.Lpad, nullptr, yhi, ylo, gemm_err,
+                                   ps)))
           return rc;
       } else {
         float* yf = reinterpret_cast<float*>(base + pl.yf);
-        if ((rc = launch_temporal(d.X, r.W, r.C, d.L, r.P, r.nt, rp.Q, bp.Lpad, yf, nullptr, nullptr, ps)))
+        if ((rc = launch_temporal(d.X, r.W, r.C, d.L, r.P, r.nt, rp.Q, bp.Lpad, yf, nullptr, nullptr,
+                                   nullptr, ps)))
           return rc;
         if ((rc = sgemm_tn(reinterpret_cast<const float*>(base + rp.uf), yf, Bt, r.K, d.L, rp.Q, 0, ps,
                            true)))

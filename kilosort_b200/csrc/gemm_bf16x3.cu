@@ -310,6 +310,23 @@ int make_bf16_map(CUtensorMap* map, const __nv_bfloat16* ptr, int64_t rows, int6
   return make_map(map, ptr, rows, cols, box_rows);
 }
 
+int make_bf16_store_map(CUtensorMap* map, const __nv_bfloat16* ptr, int64_t rows, int64_t cols,
+                        int64_t row_stride, int box_cols, int box_rows) {
+  EncodeTiled fn = encode_fn();
+  if (!fn) return fail(KS_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  if ((reinterpret_cast<uintptr_t>(ptr) & 15) || (row_stride * 2) % 16 || (box_cols * 2) % 16)
+    return fail(KS_ERR_ARG, "tensor map: 16-byte alignment needed");
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)row_stride * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(ptr), dims,
+                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(KS_ERR_CUDA, "cuTensorMapEncodeTiled failed (store map)");
+  return KS_OK;
+}
+
 int gemm_tile_n() { return kBN; }
 int gemm_tile_m() { return kBM; }
 

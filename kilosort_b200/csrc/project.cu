@@ -379,7 +379,12 @@ int launch_reorder_templates(const float* U, int64_t K, int64_t P, int64_t C, in
 
 int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
                     int64_t P, int64_t nt, int64_t Q, int64_t Lpad, float* Yf,
-                    __nv_bfloat16* Yhi, __nv_bfloat16* Ylo, cudaStream_t stream) {
+                    __nv_bfloat16* Yhi, __nv_bfloat16* Ylo, int* err, cudaStream_t stream) {
+  if (Yhi && Ylo && !Yf && err) {
+    const int rc = launch_temporal_split_tc(X, W, C, L, P, nt, Q, Lpad, Yhi, Ylo, err, stream);
+    if (rc == KS_OK) return zero_q_padding(C, P, Q, Lpad, Yf, Yhi, Ylo, stream);
+    if (rc != KS_ERR_UNSUPPORTED) return rc;
+  }
   const size_t smem = temporal_smem((int)nt, (int)P);
   const int tiles_t = (int)(Lpad / kTT);
   const long long n_tiles = (long long)tiles_t * ((C + kCG - 1) / kCG);
@@ -459,7 +464,7 @@ int launch_project(const float* X, const float* U, const float* W, int64_t C,
     ks_reorder_templates_kernel<<<reorder_blocks, 256, 0, stream>>>(
         U, (int)K, (int)P, (int)C, (int)lay.Kpad, (int)lay.Q, Uq, nullptr, nullptr);
     KS_CUDA(cudaGetLastError());
-    int rc = launch_temporal(X, W, C, L, P, nt, lay.Q, lay.Lpad, Yt, nullptr, nullptr, stream);
+    int rc = launch_temporal(X, W, C, L, P, nt, lay.Q, lay.Lpad, Yt, nullptr, nullptr, nullptr, stream);
     if (rc) return rc;
     rc = sgemm_tn(Uq, Yt, B, K, L, lay.Q, ldb, stream, tiled);
     if (rc) return rc;
@@ -475,7 +480,7 @@ int launch_project(const float* X, const float* U, const float* W, int64_t C,
   ks_reorder_templates_kernel<<<reorder_blocks, 256, 0, stream>>>(
       U, (int)K, (int)P, (int)C, (int)lay.Kpad, (int)lay.Q, nullptr, Uhi, Ulo);
   KS_CUDA(cudaGetLastError());
-  int rc = launch_temporal(X, W, C, L, P, nt, lay.Q, lay.Lpad, nullptr, Yhi, Ylo, stream);
+  int rc = launch_temporal(X, W, C, L, P, nt, lay.Q, lay.Lpad, nullptr, Yhi, Ylo, err, stream);
   if (rc) return rc;
   rc = gemm_bf16x3(Uhi, Ulo, Yhi, Ylo, B, K, L, lay.Q, lay.Kpad, lay.Lpad, ldb, tiled, err, stream);
   if (rc) return rc;

@@ -16,6 +16,10 @@ int launch_gemm_group(GemmGroup& g, cudaStream_t stream);
 // Tensor map of a bf16 [rows][cols] operand, boxes of box_rows x 64.
 int make_bf16_map(CUtensorMap* map, const __nv_bfloat16* ptr, int64_t rows, int64_t cols,
                   int box_rows);
+// Tensor map of a bf16 [rows][cols] array with a row stride (elements), no
+// swizzle, boxes of box_rows x box_cols: the destination of TMA stores.
+int make_bf16_store_map(CUtensorMap* map, const __nv_bfloat16* ptr, int64_t rows, int64_t cols,
+                        int64_t row_stride, int box_cols, int box_rows);
 int gemm_tile_n();
 int gemm_tile_m();
 
@@ -34,9 +38,16 @@ int launch_reorder_templates(const float* U, int64_t K, int64_t P, int64_t C, in
                              int64_t Q, float* Uf, __nv_bfloat16* Uhi, __nv_bfloat16* Ulo,
                              cudaStream_t stream);
 // X [C,L] -> Y [Lpad][Q] rows (f32 and/or bf16 hi/lo); Y is written for rows < Lpad.
+// The split form alone (Yhi/Ylo without Yf) runs on the tensor cores when the
+// shape allows it and err (the device error word of its bounded waits) is given.
 int launch_temporal(const float* X, const float* W, int64_t C, int64_t L, int64_t P,
                     int64_t nt, int64_t Q, int64_t Lpad, float* Yf, __nv_bfloat16* Yhi,
-                    __nv_bfloat16* Ylo, cudaStream_t stream);
+                    __nv_bfloat16* Ylo, int* err, cudaStream_t stream);
+// Split-BF16 temporal projection on tcgen05 (temporal_tc.cu); KS_ERR_UNSUPPORTED
+// (nothing launched) for shapes it does not cover (odd P, P > 8, nt > 121).
+int launch_temporal_split_tc(const float* X, const float* W, int64_t C, int64_t L, int64_t P,
+                             int64_t nt, int64_t Q, int64_t Lpad, __nv_bfloat16* Yhi,
+                             __nv_bfloat16* Ylo, int* err, cudaStream_t stream);
 int zero_q_padding(int64_t C, int64_t P, int64_t Q, int64_t Lpad, float* Yf, __nv_bfloat16* Yhi,
                    __nv_bfloat16* Ylo, cudaStream_t stream);
 // B is written row-major [K, ldb] or, when tiled, in 32-column blocks

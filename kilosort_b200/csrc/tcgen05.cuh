@@ -36,19 +36,23 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 // Bounded wait for the phase of the given parity; false (and the error word
-// set) when it runs out or another thread has set the error word.
+// set) when it runs out or another thread has set the error word.  The error
+// word (a global load) and the clock are read every 256 polls only, so a
+// waiter wakes within one poll of the phase completing.
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, int* err,
                                                   unsigned long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = ks_globaltimer();
-  while (!mbar_try_wait(bar, parity)) {
-    if (ks_ld_volatile(err) != 0) return false;
-    if (ks_globaltimer() - t0 > limit_ns) {
-      atomicCAS(err, 0, KS_ERR_TIMEOUT);
-      return false;
+  for (uint32_t spin = 1;; ++spin) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((spin & 255u) == 0u) {
+      if (ks_ld_volatile(err) != 0) return false;
+      if (ks_globaltimer() - t0 > limit_ns) {
+        atomicCAS(err, 0, KS_ERR_TIMEOUT);
+        return false;
+      }
     }
   }
-  return true;
 }
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
@@ -79,7 +83,7 @@ __device__ __forceinline__ uint64_t make_smem_desc(uint32_t addr, uint32_t lbo, 
 
 // Instruction descriptor of kind::f16 with BF16 A and B (both K-major) and an
 // FP32 accumulator: N in bits 17-22 (N >> 3), M in bits 24-28 (M >> 4).
-constexpr uint32_t idesc_bf16_f32(int M, int N) {
+__host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
 }
