@@ -283,6 +283,31 @@ KS_API int ks_whiten_int16(const int16_t* raw, int64_t T, int64_t C, int64_t ld_
                            void* stream);
 
 /*
+ * Preprocessing of one raw int16 batch (the padded window, file layout
+ * raw[t * ld_raw + ch], t < L), as kilosort/io.py:994-1026 (BinaryFiltered.filter):
+ *   X = raw[:, chan_map] (C channels; chan_map NULL: the first C), negated when
+ *   invert_sign; minus each channel's mean over the batch; minus each sample's
+ *   lower median over channels when do_car; the circular high-pass
+ *   X'[c, n] = sum_j hp_taps[j] X[c, (n + j - hp_centre) mod L] (the centre
+ *   taps of the reference's filter, 1 <= ntaps <= min(1023, L), hp_centre the
+ *   centre tap's index less the filter's offset from L/2; NULL: none); all
+ *   zeros when artifact_threshold is finite and any |X'| >= it; then
+ *   X = whiten @ X' (f32 [C][C] on the device, the drift matrix folded in by
+ *   the caller; NULL: no whitening).  Output X [C][ldx] f32.  flags (device
+ *   int[2]): [0] KS_OK, KS_ERR_ARG (a chan_map entry outside [0, ld_raw)) or
+ *   the contraction's device error; [1] 1 when the artifact test zeroed the
+ *   batch.  C <= 1024.
+ */
+KS_API size_t ks_preprocess_workspace_size(int64_t L, int64_t C, int whiten);
+KS_API int ks_preprocess_int16(const int16_t* raw, int64_t L, int64_t ld_raw,
+                               const int64_t* chan_map, int64_t C, int invert_sign,
+                               int do_car, const float* hp_taps, int64_t ntaps,
+                               int64_t hp_centre, float artifact_threshold,
+                               const float* whiten, float* X,
+                               int64_t ldx, int* flags, void* workspace,
+                               size_t workspace_bytes, void* stream);
+
+/*
  * Output consumers of extract: per spike s (template templ[s], features
  * tF [N, nC, P] as extract returns them), the position estimate
  *   w_i = m_i ||tF[s,i,:]|| / sum_j m_j ||tF[s,j,:]||, m_i = iCC_mask[i, iU[k]]

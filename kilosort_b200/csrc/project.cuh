@@ -48,6 +48,10 @@ int launch_temporal(const float* X, const float* W, int64_t C, int64_t L, int64_
 int launch_temporal_split_tc(const float* X, const float* W, int64_t C, int64_t L, int64_t P,
                              int64_t nt, int64_t Q, int64_t Lpad, __nv_bfloat16* Yhi,
                              __nv_bfloat16* Ylo, int* err, cudaStream_t stream);
+// scale * W [C][C] -> bf16 hi/lo [Cpad][Cq] (zero padded): the A operand of a
+// split-BF16 contraction over channels (whiten.cu).
+int launch_matrix_split(const float* W, int64_t C, float scale, int64_t Cpad, int64_t Cq,
+                        __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t stream);
 int zero_q_padding(int64_t C, int64_t P, int64_t Q, int64_t Lpad, float* Yf, __nv_bfloat16* Yhi,
                    __nv_bfloat16* Ylo, cudaStream_t stream);
 // B is written row-major [K, ldb] or, when tiled, in 32-column blocks

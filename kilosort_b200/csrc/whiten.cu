@@ -75,6 +75,18 @@ WhitenLayout whiten_layout(int64_t T, int64_t C) {
 
 }  // namespace
 
+namespace ks {
+
+int launch_matrix_split(const float* W, int64_t C, float scale, int64_t Cpad, int64_t Cq,
+                        __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t stream) {
+  const int g = (int)std::min<int64_t>(4096, (Cpad * Cq + 255) / 256);
+  ks_wrot_split_kernel<<<g, 256, 0, stream>>>(W, (int)C, scale, (int)Cpad, (int)Cq, hi, lo);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
+}  // namespace ks
+
 extern "C" KS_API size_t ks_whiten_int16_workspace_size(int64_t T, int64_t C) {
   if (T < 1 || C < 1) return 0;
   return whiten_layout(T, C).bytes;
@@ -100,13 +112,12 @@ extern "C" KS_API int ks_whiten_int16(const int16_t* raw, int64_t T, int64_t C, 
   __nv_bfloat16* yhi = reinterpret_cast<__nv_bfloat16*>(base + w.yhi);
   __nv_bfloat16* ylo = reinterpret_cast<__nv_bfloat16*>(base + w.ylo);
   KS_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
-  const int gu = (int)std::min<int64_t>(4096, (w.Cpad * w.Cq + 255) / 256);
-  ks_wrot_split_kernel<<<gu, 256, 0, s>>>(Wrot, (int)C, scale, (int)w.Cpad, (int)w.Cq, uhi, ulo);
-  KS_CUDA(cudaGetLastError());
+  int rc = launch_matrix_split(Wrot, C, scale, w.Cpad, w.Cq, uhi, ulo, s);
+  if (rc) return rc;
   const int gy = (int)std::min<int64_t>(8192, (w.Tpad * w.Cq + 255) / 256);
   ks_raw_split_kernel<<<gy, 256, 0, s>>>(raw, T, (int)C, ld_raw, (int)w.Cq, w.Tpad, yhi, ylo);
   KS_CUDA(cudaGetLastError());
-  int rc = gemm_bf16x3(uhi, ulo, yhi, ylo, X, C, T, w.Cq, w.Cpad, w.Tpad, ldx, false, err, s);
+  rc = gemm_bf16x3(uhi, ulo, yhi, ylo, X, C, T, w.Cq, w.Cpad, w.Tpad, ldx, false, err, s);
   if (rc) return rc;
   KS_CUDA(cudaMemcpyAsync(status, err, sizeof(int), cudaMemcpyDeviceToDevice, s));
   return KS_OK;

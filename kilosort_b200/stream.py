@@ -10,8 +10,11 @@ ends early (the last) is padded with its last sample.  Per group of batches:
   page-locked source (the recording's memory is registered once; the two
   edge windows are assembled in a small page-locked staging buffer);
 * compute stream: ``ks_whiten_int16`` (X = scale * Wrot @ raw, split-BF16 on
-  the tensor cores) writes each batch into a ``BatchedMatcher``'s inputs, then
-  its captured graph matches the group (grouped contraction, team-split peel);
+  the tensor cores) -- or, with ``preprocess`` settings (chan_map, hp_filter,
+  do_CAR, invert_sign, artifact_threshold), the whole batch filter of
+  kilosort/io.py:994-1026 (``ks_preprocess_int16``) -- writes each batch into
+  a ``BatchedMatcher``'s inputs, then its captured graph matches the group
+  (grouped contraction, team-split peel);
 * two matchers alternate, so the host reads one group's spikes while the GPU
   matches the next;
 * every ``refine_every`` groups the templates take one gradient step on the
@@ -28,6 +31,7 @@ import torch
 from . import _lib
 from .adjoint import reconstruction_loss
 from .batched import BatchedMatcher, Recording
+from .preprocess import Preprocessor
 from .template_matching import _ptr, _stream, prepare_matching
 
 
@@ -74,16 +78,20 @@ class Whitener:
         lib = _lib.load()
         self.ws = torch.empty(lib.ks_whiten_int16_workspace_size(L, self.C), dtype=torch.uint8,
                               device=device)
-        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        self.flags = torch.zeros(1, dtype=torch.int32, device=device)
 
     def __call__(self, raw_dev: torch.Tensor, X: torch.Tensor):
         T, C = raw_dev.shape
         lib = _lib.load()
         _lib.check(lib.ks_whiten_int16(_ptr(raw_dev), T, C, raw_dev.stride(0), _ptr(self.Wrot),
-                                       self.scale, _ptr(X), X.stride(0), _ptr(self.status),
+                                       self.scale, _ptr(X), X.stride(0), _ptr(self.flags),
                                        _ptr(self.ws), self.ws.numel(), _stream(X.device)),
                    "ks_whiten_int16")
         return X
+
+    def status(self):
+        """(device status, artifact) of the last call (synchronises)."""
+        return int(self.flags.item()), False
 
 
 class StreamMatcher:
@@ -91,7 +99,8 @@ class StreamMatcher:
 
     def __init__(self, raw: np.ndarray, Wrot: torch.Tensor, scale: float, ops, U: torch.Tensor,
                  NT: int, group: int = 8, teams: Optional[int] = 0, projection: str = "bf16x3",
-                 refine_every: int = 0, refine_lr: float = 1e-4, device=None):
+                 refine_every: int = 0, refine_lr: float = 1e-4, device=None,
+                 preprocess: Optional[dict] = None):
         if raw.dtype != np.int16 or raw.ndim != 2:
             raise TypeError("raw must be an int16 [samples, channels] array")
         self.raw = np.ascontiguousarray(raw)
@@ -106,7 +115,13 @@ class StreamMatcher:
         self.rec = Recording.from_ops(ops, U, self.ctc)
         self.windows = batch_windows(raw.shape[0], self.NT, self.nt)
         self.n_batches = len(self.windows)
-        self.whiten = Whitener(Wrot, scale, self.L, self.device)
+        if preprocess is None:
+            self.whiten = Whitener(Wrot, scale, self.L, self.device)
+        else:
+            # the whole filter of kilosort/io.py:994-1026 on each padded batch
+            W = torch.as_tensor(Wrot, dtype=torch.float32) * float(scale)
+            self.whiten = Preprocessor(self.C, self.L, whiten=W, device=self.device,
+                                       **preprocess)
         self.refine_every = int(refine_every)
         self.refine_lr = float(refine_lr)
         self.refinements = 0
@@ -246,6 +261,9 @@ class StreamMatcher:
                 collect(g - 1)
         if groups:
             collect(len(groups) - 1)
+        code, _ = self.whiten.status()
+        if code != _lib.KS_OK:
+            raise _lib.KilosortB200Error(code, f"stream: whitening device status {code}")
         cat = (lambda xs, dt: np.concatenate(xs).astype(dt) if xs else np.zeros(0, dt))
         return (cat(times, np.int64), cat(templ, np.int64), cat(amps, np.float32),
                 cat(bidx, np.int64))

@@ -314,3 +314,33 @@ class SyntheticBinary:
         import torch
         x = np.ascontiguousarray(self.rec.batch(int(ibatch)))
         return torch.from_numpy(x).to(self.device)
+
+
+def raw_batch(seed: int, n_chan_bin: int, L: int, fs: float = 30000.0,
+              n_spikes: int = 40) -> np.ndarray:
+    """A raw int16 batch in the file layout [L, n_chan_bin], with what the
+    preprocessing removes: per-channel offsets (-500..500), a slow per-channel
+    drift (1-8 Hz, amplitude 20-120), a common-mode signal on every channel
+    (amplitude 60, 50 Hz plus noise), white noise (sd 20) and negative spikes
+    (amplitude 80-300, trough 0.3 ms wide, on 3 neighbouring channels)."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(L) / fs
+    off = rng.uniform(-500, 500, n_chan_bin)
+    f_drift = rng.uniform(1, 8, n_chan_bin)
+    a_drift = rng.uniform(20, 120, n_chan_bin)
+    ph = rng.uniform(0, 2 * np.pi, n_chan_bin)
+    common = 60 * np.sin(2 * np.pi * 50 * t) + 15 * rng.standard_normal(L)
+    x = (off[None, :] + a_drift[None, :] * np.sin(2 * np.pi * f_drift[None, :] * t[:, None]
+                                                   + ph[None, :])
+         + common[:, None] + 20 * rng.standard_normal((L, n_chan_bin)))
+    w = np.exp(-0.5 * ((np.arange(-15, 16)) / 4.5) ** 2)
+    for _ in range(n_spikes):
+        s = int(rng.integers(20, max(21, L - 20)))
+        c = int(rng.integers(0, n_chan_bin))
+        a = rng.uniform(80, 300)
+        for dc, g in ((-1, 0.5), (0, 1.0), (1, 0.5)):
+            cc = c + dc
+            if 0 <= cc < n_chan_bin:
+                lo, hi = max(0, s - 15), min(L, s + 16)
+                x[lo:hi, cc] -= a * g * w[lo - (s - 15):hi - (s - 15)]
+    return np.clip(np.round(x), -32768, 32767).astype(np.int16)

@@ -20,6 +20,7 @@ per batch (default 100000, the reference's fixed buffer size).
 from __future__ import annotations
 
 import logging
+import weakref
 
 import numpy as np
 import torch
@@ -92,25 +93,26 @@ class _TransposedCtc:
 
     `extract` matches every batch with the same ctc tensor; transposing it once
     instead of per batch saves a full pass over K*K*(2nt+1) floats per batch.
-    The entry is keyed by storage address, shape and the tensor's version
-    counter, so an in-place change of ctc invalidates it.
+    The entry belongs to that tensor object (a weak reference: a new tensor
+    that happens to reuse the freed storage of an old one is a new entry) and
+    to its version counter, so an in-place change of ctc invalidates it.
     """
 
     def __init__(self):
-        self._key = None
+        self._ref = None
+        self._version = None
         self._val = None
 
     def get(self, ctc: torch.Tensor, nt: int) -> torch.Tensor:
-        key = (ctc.data_ptr(), tuple(ctc.shape), ctc.device, ctc._version)
-        if self._key == key:
+        if self._ref is not None and self._ref() is ctc and self._version == ctc._version:
             return self._val
-        self._key, self._val = None, None
+        self._ref, self._version, self._val = None, None, None
         K = ctc.shape[0]
         out = torch.empty_like(ctc)
         lib = _lib.load()
         _lib.check(lib.ks_ctc_transpose(_ptr(ctc), K, nt, _ptr(out), _stream(ctc.device)),
                    "ks_ctc_transpose")
-        self._key, self._val = key, out
+        self._ref, self._version, self._val = weakref.ref(ctc), ctc._version, out
         return out
 
 

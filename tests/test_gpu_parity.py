@@ -244,3 +244,23 @@ def test_tiled_scores_and_transposed_ctc(cuda_device):
     ctc = torch.from_numpy(g["ctc_full"]).to(DEV)
     ctcT = kb.transpose_ctc(ctc, 61)
     assert torch.equal(ctcT, ctc.transpose(0, 1))
+
+
+def test_transposed_ctc_cache_follows_the_tensor(cuda_device):
+    """run_matching keeps the transposed ctc of the last ctc tensor it saw; a
+    new ctc of the same shape that reuses the freed storage of the previous
+    one (the caching allocator hands the block straight back) must not be
+    taken for it.  Each result equals the oracle's for its own templates."""
+    recs = [synth.make_recording(8101 + i, n_chan=48, n_templates=30, batch_lengths=[4000])
+            for i in range(3)]
+    for rec in recs:
+        U = torch.from_numpy(rec.U)
+        W = torch.from_numpy(rec.wPCA)
+        X = torch.from_numpy(np.ascontiguousarray(rec.batch(0)))
+        ops = dict(Th_learned=8.0, nt=rec.nt, max_peels=100, wPCA=W)
+        ctc = kb.prepare_matching(dict(ops, wPCA=W.to(DEV)), U.to(DEV))
+        st, amps, _, _ = kb.run_matching(dict(ops, wPCA=W.to(DEV)), X.to(DEV), U.to(DEV), ctc,
+                                         device=DEV)
+        st_r, amps_r, _, _ = om.run_matching(ops, X, U, ctc.cpu())
+        np.testing.assert_array_equal(st.cpu().numpy(), st_r.numpy())
+        del ctc                               # its storage goes back to the allocator

@@ -1,0 +1,119 @@
+"""Device preprocessing (ks_preprocess_int16) against the reference's filter.
+
+* the golden cases (the reference's own BinaryFiltered.filter outputs,
+  tests/golden/golden_pre.npz): max |X - X_ref| <= 1e-4 of max |X_ref| (the
+  whitening runs in split-BF16, ~2^-16 per product; the FP32 circular FIR
+  and the exact mean stay near 1e-7); the artifact case is all zeros with the
+  artifact flag set;
+* a full-size batch (385 file channels, 384 mapped, L = 60122, CAR, high-pass,
+  whitening with a drift matrix) against the oracle in float64, same bound;
+* a channel map entry outside the file's channels is reported (KS_ERR_ARG in
+  the status word), nothing is read out of bounds;
+* the stream with preprocessing equals one run_matching per preprocessed
+  padded batch.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+import torch
+
+import kilosort_b200 as kb
+from kilosort_b200 import _lib, synth
+from kilosort_b200.preprocess import Preprocessor
+from kilosort_b200.stream import StreamMatcher, batch_windows, padded_raw_window
+from oracle import preprocess as op
+from tests.golden import make_golden_pre as mk
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+G = np.load(mk.__file__.replace("make_golden_pre.py", "golden_pre.npz"))
+
+
+@pytest.mark.parametrize("name", list(mk.CASES))
+def test_golden_cases(cuda_device, name):
+    seed, L, inv, car, use_hp, use_w, shift = G[f"{name}_params"]
+    raw = synth.raw_batch(int(seed), int(G["n_chan_bin"]), int(L))
+    assert hashlib.sha256(raw.tobytes()).hexdigest()[:16] == str(G[f"{name}_raw_sha"])
+    drift = None
+    if shift >= 0:
+        drift = op.drift_matrix(G[f"{name}_xc"], G[f"{name}_yc"], float(shift)).float()
+    p = Preprocessor(int(G["n_chan_bin"]), int(L),
+                     whiten=torch.from_numpy(G[f"{name}_W"]) if use_w else None,
+                     chan_map=G["chan_map"], hp_filter=op.highpass_filter() if use_hp else None,
+                     do_CAR=bool(car), invert_sign=bool(inv),
+                     artifact_threshold=float(G[f"{name}_thr"]), device=DEV)
+    X = p(torch.from_numpy(raw).to(DEV), drift=drift).cpu().numpy()
+    status, artifact = p.status()
+    assert status == _lib.KS_OK
+    ref = G[f"{name}_out"]
+    if name == "artifact":
+        assert artifact and not X.any()
+        return
+    assert not artifact
+    err = np.abs(X - ref).max()
+    assert err <= 1e-4 * np.abs(ref).max(), (name, err, np.abs(ref).max())
+
+
+def test_full_size_with_drift(cuda_device):
+    n_bin, L = 385, 60122
+    raw = synth.raw_batch(7101, n_bin, L, n_spikes=3000)
+    cmap = np.delete(np.arange(n_bin), 200)
+    C = len(cmap)
+    rng = np.random.default_rng(3)
+    W = (np.eye(C) + 0.05 * rng.standard_normal((C, C))).astype(np.float32)
+    xc = np.tile(np.array([43.0, 11.0, 59.0, 27.0]), C // 4)
+    yc = 20.0 * (np.arange(C) // 2)
+    M = op.drift_matrix(xc, yc, 4.0)
+    hp = op.highpass_filter()
+    p = Preprocessor(n_bin, L, whiten=torch.from_numpy(W), chan_map=cmap, hp_filter=hp,
+                     device=DEV)
+    X = p(torch.from_numpy(raw).to(DEV), drift=M.float()).cpu().numpy()
+    assert p.status() == (_lib.KS_OK, False)
+    ref = op.filter_batch(torch.from_numpy(raw.T.astype(np.float64)),
+                          chan_map=torch.from_numpy(cmap), hp=hp.double(),
+                          whiten=torch.from_numpy(W).double(), drift=M.double()).numpy()
+    err = np.abs(X - ref).max()
+    assert err <= 1e-4 * np.abs(ref).max(), (err, np.abs(ref).max())
+
+
+def test_bad_channel_map_is_reported(cuda_device):
+    raw = synth.raw_batch(7102, 16, 1100)
+    p = Preprocessor(16, 1100, chan_map=np.array([0, 1, 2, 16]), device=DEV)
+    p(torch.from_numpy(raw).to(DEV))
+    assert p.status()[0] == _lib.KS_ERR_ARG
+
+
+def test_stream_with_preprocessing_equals_per_batch(cuda_device):
+    NT = 3000
+    rec = synth.make_recording(6101, n_chan=64, probe="np1", n_templates=40,
+                               batch_lengths=[NT] * 4, rate_hz=(10.0, 30.0))
+    n_bin = 66
+    cmap = np.arange(1, 65)                      # file channels 1..64
+    noise = synth.raw_batch(6102, n_bin, rec.signal.shape[1])
+    raw = noise.astype(np.float64)
+    raw[:, cmap] += np.round(25.0 * rec.signal.T)
+    raw = np.clip(raw, -32768, 32767).astype(np.int16)
+    U = torch.from_numpy(rec.U).to(DEV)
+    W = torch.from_numpy(rec.wPCA).to(DEV)
+    ops = dict(Th_learned=8.0, nt=rec.nt, max_peels=100, wPCA=W)
+    Wrot = torch.eye(64) / 25.0
+    pre = dict(chan_map=cmap, hp_filter=op.highpass_filter(), do_CAR=True)
+    sm = StreamMatcher(raw, Wrot, 1.0, ops, U, NT=NT, group=2, teams=2, preprocess=pre)
+    times, templ, amps, bidx = sm.run()
+    sm.close()
+    assert len(times) > 50
+    nt = rec.nt
+    L = NT + 2 * nt
+    p = Preprocessor(n_bin, L, whiten=Wrot, device=DEV, **pre)
+    ctc = kb.prepare_matching(ops, U)
+    ref_t, ref_k = [], []
+    for b in range(len(batch_windows(raw.shape[0], NT, nt))):
+        win = padded_raw_window(raw, b, NT, nt, np.empty((L, n_bin), np.int16))
+        X = p(torch.from_numpy(win).to(DEV))
+        st, _, _, _ = kb.run_matching(dict(ops, projection="bf16x3"), X, U, ctc, device=DEV)
+        st = st.cpu().numpy()
+        ref_t.append(st[:, 0] - nt + b * NT)
+        ref_k.append(st[:, 1])
+    np.testing.assert_array_equal(times, np.concatenate(ref_t))
+    np.testing.assert_array_equal(templ, np.concatenate(ref_k))

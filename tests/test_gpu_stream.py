@@ -35,7 +35,7 @@ def test_whitening_matches_float64(cuda_device):
     ref = (scale * Wrot.double()) @ torch.from_numpy(raw).double().T
     err = (X.double().cpu() - ref).abs().max().item() / ref.abs().max().item()
     assert err < 3e-5, err
-    assert int(w.status.item()) == 0
+    assert w.status()[0] == 0
 
 
 def _raw_recording(seed=6001, C=64, K=40, NT=3000, nb=5):
