@@ -335,14 +335,16 @@ def adjoint_main(args, dev, rank, world):
 
 STREAM = ("long dense recording, shortened: C=384 (NP1-like), K=2000 templates (amplitudes "
           "5-40 sd, 1-30 Hz), {nb} batches of 60000 samples streamed from page-locked host "
-          "int16 (channel-mixed, scale 200) through GPU whitening into the batched split-BF16 "
-          "matcher, one adjoint template-refinement step per group")
+          "int16 (channel-mixed, scale 200) through the GPU batch filter (mean, CAR median, "
+          "300 Hz high-pass, whitening) into the batched split-BF16 matcher, one adjoint "
+          "template-refinement step per group")
 
 
 def stream_main(args, dev, rank, world):
     """Config 5 on a shortened recording: host int16 -> results on the host."""
     import kilosort_b200 as kb  # noqa: F401
     from kilosort_b200 import synth
+    from kilosort_b200.preprocess import highpass_filter
     from kilosort_b200.stream import StreamMatcher
     nb = args.batches if args.batches != 20 else 8
     rec = synth.make_recording(1005, n_chan=384, probe="np1", n_templates=2000,
@@ -363,8 +365,10 @@ def stream_main(args, dev, rank, world):
     W = torch.from_numpy(rec.wPCA).to(dev)
     ops = dict(Th_learned=TH, nt=NT, max_peels=100, wPCA=W)
     U = U0.clone()
+    # the whole batch filter of the reference (mean, CAR, high-pass, whitening)
+    pre = dict(hp_filter=highpass_filter(), do_CAR=True)
     sm = StreamMatcher(raw, Wrot, 1.0 / 200.0, ops, U, NT=NT_BATCH, group=args.group_stream,
-                       teams=None, refine_every=1, refine_lr=1e-7)
+                       teams=None, refine_every=1, refine_lr=1e-7, preprocess=pre)
     for _ in range(max(1, args.warmup)):
         sm.run()
     torch.cuda.synchronize()
@@ -386,7 +390,8 @@ def stream_main(args, dev, rank, world):
         "metric": "channel-samples/s", "value": value, "unit": "channel-samples/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "int16 in, f32 (split-bf16 whitening and projection)", "data": "synthetic",
+        "dtype": "int16 in, f32 (f32 filter, split-bf16 whitening and projection)",
+        "data": "synthetic",
         "config": {"workload": STREAM.format(nb=nb), "batches": sm.n_batches,
                    "group": sm.group, "teams": sm.matchers[0].teams,
                    "refinements_per_step": sm.refinements // (args.steps + max(1, args.warmup)),
@@ -395,10 +400,11 @@ def stream_main(args, dev, rank, world):
                    "parallelism": f"replicas x{world}"},
         "spikes_per_step": nsp,
         "spikes_per_s": nsp * world / dt,
-        # per batch: matrix split, raw split, whitening contraction, temporal
-        # projection; per group: energy, {nm, 1/nm}, reorder, contraction,
-        # peel; per refinement: loss (5), adjoint (6), ctc (3), transpose (1)
-        "gpu_launches": (4 * sm.n_batches + 5 * -(-sm.n_batches // sm.group)
+        # per batch: filter (sums, CAR, high-pass, matrix split, whitening
+        # contraction, artifact zeroing), temporal projection; per group:
+        # energy, {nm, 1/nm}, reorder, contraction, peel; per refinement: loss
+        # (5), adjoint (6), ctc (3), transpose (1)
+        "gpu_launches": (7 * sm.n_batches + 5 * -(-sm.n_batches // sm.group)
                          + 15 * (sm.refinements // (args.steps + max(1, args.warmup)))),
         "e2e": {"value": value, "unit": "channel-samples/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": nsp * 20},

@@ -267,6 +267,19 @@ KS_API int ks_recon_adjoint(const float* Xres, const int64_t* st, const float* a
                             void* stream);
 
 /*
+ * Template similarity, sim[i, j] = max over lags l of
+ *   sum_{k,m} (sum_c Wn[i,c,k] Wn[j,c,m]) * WtW[k,m,l],  Wn = Wall / (1e-6 + ||Wall||),
+ * with WtW the flipped full cross-correlation of the wPCA rows (as ks_ctc).
+ * Wall [K, C, P] (the clustering's layout), W [P, nt], sim [K, K], all f32.
+ * Replaces kilosort/CCG.py:94-102 (similarity, used for Phy's
+ * similar_templates at kilosort/io.py:377); the lags are never stored.
+ */
+KS_API size_t ks_similarity_workspace_size(int64_t K, int64_t C, int64_t P, int64_t nt);
+KS_API int ks_similarity(const float* Wall, const float* W, int64_t K, int64_t C, int64_t P,
+                         int64_t nt, float* sim, void* workspace, size_t workspace_bytes,
+                         void* stream);
+
+/*
  * Whitening of raw int16 samples (the streaming front end):
  *   X[c, t] = sum_c' Wrot[c, c'] * scale * raw[t * ld_raw + c']   (t < T, c < C)
  * with raw in the recording's layout (samples x channels), X row-major

@@ -6,6 +6,8 @@
   its template's peak channel (channels beyond ``position_limit`` weigh 0).
 * ``spike_amplitudes(tF)`` -- the Phy-export amplitudes of kilosort/io.py:353,
   ``||tF[s]||`` (float32 numpy).
+* ``template_similarity(Wall, W, nt)`` -- kilosort/CCG.py:94-102, Phy's
+  similar_templates (io.py:377), on the device (kernel ``ks_similarity``).
 
 ``st`` and ``tF`` may be the host arrays `extract` returns; they are moved to
 the device of ``ops['iU']`` (which must be a CUDA device).
@@ -65,3 +67,29 @@ def spike_amplitudes(tF, ops):
     st = np.zeros((torch.as_tensor(tF).shape[0], 2))
     _, _, amps = _positions(st, tF, ops)
     return amps.cpu().numpy()
+
+
+def template_similarity(Wall: torch.Tensor, W: torch.Tensor, nt: int = 61,
+                        to_host: bool = True):
+    """Same inputs and output as kilosort/CCG.py:94-102 (``similarity``):
+    ``Wall`` [K, C, P] templates, ``W`` = wPCA [P, nt]; returns [K, K] float32,
+    the maximum over lags of the cross-correlation of the unit-norm templates
+    (numpy on the host, as the reference returns it, unless ``to_host`` is
+    False).  Runs on the device of ``Wall`` (``ks_similarity``)."""
+    if not isinstance(Wall, torch.Tensor) or Wall.device.type != "cuda":
+        raise ValueError("Wall must be a CUDA tensor (this path has no CPU fallback)")
+    dev = Wall.device
+    Wd = Wall.to(torch.float32).contiguous()
+    Wp = W.to(device=dev, dtype=torch.float32).contiguous()
+    K, C, P = Wd.shape
+    lib = _lib.load()
+    ws = torch.empty(lib.ks_similarity_workspace_size(K, C, P, nt), dtype=torch.uint8, device=dev)
+    sim = torch.empty((K, K), dtype=torch.float32, device=dev)
+    _lib.check(lib.ks_similarity(_ptr(Wd), _ptr(Wp), K, C, P, nt, _ptr(sim), _ptr(ws),
+                                 ws.numel(), _stream(dev)), "ks_similarity")
+    return sim.cpu().numpy() if to_host else sim
+
+
+def template_amplitudes(Wall: torch.Tensor) -> np.ndarray:
+    """kilosort/io.py:378: ``||Wall[k]||`` over channels and components."""
+    return torch.norm(Wall, dim=[-2, -1]).cpu().numpy()

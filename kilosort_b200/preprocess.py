@@ -28,6 +28,19 @@ def _ptr(t) -> int:
     return 0 if t is None else t.data_ptr()
 
 
+def highpass_filter(fs: float = 30000, cutoff: float = 300) -> torch.Tensor:
+    """The reference's time-domain high-pass (kilosort/preprocessing.py:121-136):
+    the response of a 3rd-order Butterworth high-pass run forwards and
+    backwards (scipy ``filtfilt``) to a unit impulse at the centre of 30122
+    samples, float32."""
+    from scipy.signal import butter, filtfilt
+    n = 30122
+    b, a = butter(3, cutoff, fs=fs, btype="high")
+    x = np.zeros(n)
+    x[n // 2] = 1
+    return torch.from_numpy(filtfilt(b, a, x).copy()).float()
+
+
 def highpass_taps(hp_filter, L: int, ntaps: int = 1023):
     """(taps float32 [n], centre): X'[n] = sum_j taps[j] X[(n + j - centre) mod L].
 

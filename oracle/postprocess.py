@@ -6,7 +6,10 @@ TEST INFRASTRUCTURE ONLY.  Restates with the same PyTorch ops:
   (compute_spike_positions): per spike, the 2-norm of its PC features on each
   of the nC channels nearest its template's peak channel, masked by
   ``iCC_mask``, normalised to sum 1, weights the channels' x and y;
-* ``amplitudes`` -- kilosort/io.py:353: the 2-norm of each spike's features.
+* ``amplitudes`` -- kilosort/io.py:353: the 2-norm of each spike's features;
+* ``similarity`` -- kilosort/CCG.py:94-102: the maximum over lags of the
+  cross-correlation of the unit-norm templates (UtU over channels, WtW the
+  flipped full cross-correlation of the wPCA rows).
 
 Pinned against tests/golden/golden_post.npz (the reference's own outputs).
 """
@@ -29,3 +32,13 @@ def spike_positions(st, tF, iCC, iCC_mask, iU, xc, yc):
 
 def amplitudes(tF):
     return torch.norm(tF, dim=[-2, -1]).numpy()
+
+
+def similarity(Wall, W, nt=61):
+    from torch.nn.functional import conv1d
+    WtW = conv1d(W.reshape(-1, 1, nt), W.reshape(-1, 1, nt), padding=nt)
+    WtW = torch.flip(WtW, [2])
+    mu = (Wall ** 2).sum((1, 2), keepdims=True) ** .5
+    Wnorm = Wall / (1e-6 + mu)
+    UtU = torch.einsum('ilk, jlm -> ijkm', Wnorm, Wnorm)
+    return torch.einsum('ijkm, kml -> ijl', UtU, WtW).numpy().max(axis=-1)

@@ -9,7 +9,9 @@ Loads the golden `extract` case (tests/golden/golden_extract.npz, its
 recording regenerated from the stored seed), and runs the reference's
 ``postprocessing.compute_spike_positions`` (kilosort/postprocessing.py:33-62)
 and the Phy-export amplitudes ``torch.norm(tF, dim=[-2, -1])``
-(kilosort/io.py:353) on it.  ``kilosort.clustering_qr`` (which needs faiss)
+(kilosort/io.py:353) on it; and the reference's template similarity
+``CCG.similarity`` (kilosort/CCG.py:94-102, io.py:377) on that case's
+templates in the clustering's layout (Wall = U transposed to [K, C, P]).  ``kilosort.clustering_qr`` (which needs faiss)
 is replaced by an empty stub: compute_spike_positions does not use it.
 Writes tests/golden/golden_post.npz.
 """
@@ -36,13 +38,13 @@ def load_reference(path):
     stub.xy_templates = None
     stub.get_data_cpu = None
     sys.modules["kilosort.clustering_qr"] = stub
-    from kilosort import postprocessing, template_matching
-    return postprocessing, template_matching
+    from kilosort import postprocessing, template_matching, CCG
+    return postprocessing, template_matching, CCG
 
 
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    post, tm = load_reference(ref)
+    post, tm, ccg = load_reference(ref)
     g = np.load(os.path.join(HERE, "golden_extract.npz"))
     rec = synth.make_recording(**ast.literal_eval(str(g["seed_kwargs"])))
     U = torch.from_numpy(rec.U)
@@ -53,6 +55,9 @@ if __name__ == "__main__":
     tF = torch.from_numpy(g["tF"])
     xs, ys = post.compute_spike_positions(st, tF, ops)
     amplitudes = torch.norm(tF, dim=[-2, -1]).cpu().numpy()
+    Wall = U.transpose(1, 2).contiguous()
+    sim = ccg.similarity(Wall, torch.from_numpy(rec.wPCA).contiguous(), nt=rec.nt)
     np.savez_compressed(os.path.join(HERE, "golden_post.npz"), xs=xs, ys=ys,
-                        amplitudes=amplitudes, iCC_mask=iCC_mask.numpy())
+                        amplitudes=amplitudes, iCC_mask=iCC_mask.numpy(),
+                        similarity=sim.astype(np.float32))
     print(f"post: {len(xs)} spikes")

@@ -1,6 +1,9 @@
 """Spike positions and amplitudes on the GPU (ks_spike_positions) against the
 reference's own outputs on the golden extract case (positions within 1e-4 um,
-amplitudes within 1e-6 relative: the kernel's norms sum in another order)."""
+amplitudes within 1e-6 relative: the kernel's norms sum in another order), and
+the template similarity (ks_similarity) against the reference's CCG.similarity
+(within 1e-5 of the largest entry: FP32 sums in another order), also at
+C=384 / K=600 against the oracle."""
 import ast
 import os
 
@@ -58,3 +61,25 @@ def test_bad_template_index_is_reported(cuda_device):
     st[0, 1] = 10 ** 6
     with pytest.raises(kb._lib.KilosortB200Error):
         postprocess.compute_spike_positions(st, torch.from_numpy(g["tF"]), ops)
+
+
+def test_similarity_matches_reference(cuda_device):
+    g = gu.load("extract")
+    post = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_post.npz"))
+    rec = synth.make_recording(**ast.literal_eval(str(g["seed_kwargs"])))
+    Wall = torch.from_numpy(rec.U).transpose(1, 2).contiguous().to(DEV)
+    sim = postprocess.template_similarity(Wall, torch.from_numpy(rec.wPCA).to(DEV), rec.nt)
+    ref = post["similarity"]
+    assert np.abs(sim - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+def test_similarity_cfg2_templates(cuda_device):
+    rec = synth.config_recording(2, n_batches=1)
+    Wall = torch.from_numpy(rec.U).transpose(1, 2).contiguous()
+    W = torch.from_numpy(rec.wPCA)
+    sim = postprocess.template_similarity(Wall.to(DEV), W.to(DEV), rec.nt)
+    ref = op.similarity(Wall, W, rec.nt)
+    assert sim.shape == (600, 600)
+    assert np.abs(sim - ref).max() <= 1e-5 * np.abs(ref).max()
+    # each template is most similar to itself (unit norm: about 1 at lag 0)
+    assert np.all(np.abs(np.diag(sim) - 1) < 1e-3)

@@ -82,7 +82,8 @@ def test_extract_features_bit_exact():
 
 
 def test_output_consumers_bit_exact():
-    """Oracle positions and amplitudes equal the reference's on the golden extract."""
+    """Oracle positions, amplitudes and template similarity equal the reference's
+    on the golden extract case."""
     from kilosort_b200 import synth
     from oracle import postprocess as op
     g = gu.load("extract")
@@ -95,3 +96,6 @@ def test_output_consumers_bit_exact():
     np.testing.assert_array_equal(xs, post["xs"])
     np.testing.assert_array_equal(ys, post["ys"])
     np.testing.assert_array_equal(op.amplitudes(torch.from_numpy(g["tF"])), post["amplitudes"])
+    Wall = torch.from_numpy(rec.U).transpose(1, 2).contiguous()
+    np.testing.assert_array_equal(op.similarity(Wall, torch.from_numpy(rec.wPCA), rec.nt),
+                                  post["similarity"])
