@@ -267,6 +267,31 @@ KS_API int ks_recon_adjoint(const float* Xres, const int64_t* st, const float* a
                             void* stream);
 
 /*
+ * Universal-template spike detection on one batch X [C, L] (whitened, padded):
+ *   B = conv1d(X, wTEMP [nk, nt]) (padding nt/2), for each template position
+ *   f < Nfilt and sample t the weighted sums A[s, k] = sum_j weigh[s, j, f] *
+ *   B[iC[j, f], k, t] (iC [nC, Nfilt] int64, weigh [nsizes, nC, Nfilt]), the
+ *   largest |A| with its signed index (1 + s*nk + k) * sign, the maximum of
+ *   that over the nC2 nearest positions iC2 [nC2, Nfilt] (zero for t < nt and
+ *   t >= L - nt), a (2*nt0+1) max-pool in time, peaks above th.  Outputs in
+ *   (position, time) order, at most `capacity`: xy [cap, 2] (f, t), imax [cap]
+ *   (s*nk + k), amp [cap], adist [nC, cap], yct [cap] (yc [C] f32), tF
+ *   [cap, nC, P] (wPCA [P, nt]).  info (device int64[4]): [0] spikes written,
+ *   [1] KS_OK / KS_ERR_OVERFLOW / KS_ERR_ARG (a channel index outside [0, C)),
+ *   [3] spikes found.  nk, nsizes <= 8, nC <= 32, P <= 8.
+ *   Replaces kilosort/spikedetect.py:133-197 (template_match, yweighted) and
+ *   the features of run() (:265-266).
+ */
+KS_API size_t ks_detect_workspace_size(int64_t C, int64_t L, int64_t nk, int64_t Nfilt);
+KS_API int ks_detect(const float* X, int64_t C, int64_t L, const float* wTEMP, int64_t nk,
+                     int64_t nt, const int64_t* iC, int64_t nC, const int64_t* iC2,
+                     int64_t nC2, const float* weigh, int64_t nsizes, int64_t Nfilt,
+                     int64_t nt0, float th, const float* wPCA, int64_t P, const float* yc,
+                     int64_t capacity, int64_t* xy, int64_t* imax, float* amp, float* adist,
+                     float* yct, float* tF, int64_t* info, void* workspace,
+                     size_t workspace_bytes, void* stream);
+
+/*
  * Template similarity, sim[i, j] = max over lags l of
  *   sum_{k,m} (sum_c Wn[i,c,k] Wn[j,c,m]) * WtW[k,m,l],  Wn = Wall / (1e-6 + ||Wall||),
  * with WtW the flipped full cross-correlation of the wPCA rows (as ks_ctc).

@@ -66,6 +66,10 @@ SIGNATURES = {
     "ks_recon_adjoint": (_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
                                 _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "ks_spike_positions": (_int, [_vp] * 7 + [_i64] * 5 + [_vp] * 5),
+    "ks_detect_workspace_size": (_sz, [_i64, _i64, _i64, _i64]),
+    "ks_detect": (_int, [_vp, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64,
+                         _i64, _i64, _f32, _vp, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _vp,
+                         _vp, _vp, _vp, _sz, _vp]),
     "ks_similarity_workspace_size": (_sz, [_i64, _i64, _i64, _i64]),
     "ks_similarity": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp, _sz, _vp]),
     "ks_preprocess_workspace_size": (_sz, [_i64, _i64, _int]),

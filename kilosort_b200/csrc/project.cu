@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(kTemporalThreads)
 ks_temporal_kernel(const float* __restrict__ X, const float* __restrict__ W,
                    int C, int L, int nt, int Q, int tiles_t, int n_tiles,
                    float* __restrict__ Yf, __nv_bfloat16* __restrict__ Yhi,
-                   __nv_bfloat16* __restrict__ Ylo) {
+                   __nv_bfloat16* __restrict__ Ylo, float* __restrict__ YT, long long ldyt) {
   extern __shared__ __align__(16) float sm[];
   constexpr int kS = kTT / (kTemporalThreads / kCG);   // samples per thread (8)
   const int xw = temporal_xw(nt);
@@ -172,6 +172,19 @@ ks_temporal_kernel(const float* __restrict__ X, const float* __restrict__ W,
     // the window is no longer read: the next fetch may overwrite this buffer
     __syncthreads();
     const long long q0 = (long long)(cg0 + cl) * PP;
+    if (YT) {
+      // rows (channel, component), samples contiguous: 8 samples per store pair
+      if (cg0 + cl < C) {
+#pragma unroll
+        for (int p = 0; p < PP; ++p) {
+          float4* dst = reinterpret_cast<float4*>(YT + (q0 + p) * ldyt + tau0 + g * kS);
+          dst[0] = make_float4(acc[0][p], acc[1][p], acc[2][p], acc[3][p]);
+          dst[1] = make_float4(acc[4][p], acc[5][p], acc[6][p], acc[7][p]);
+        }
+      }
+      buf ^= 1;
+      continue;
+    }
 #pragma unroll
     for (int i = 0; i < kS; ++i) {
       const long long o = (long long)(tau0 + g * kS + i) * Q + q0;
@@ -377,14 +390,10 @@ int launch_reorder_templates(const float* U, int64_t K, int64_t P, int64_t C, in
   return KS_OK;
 }
 
-int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
-                    int64_t P, int64_t nt, int64_t Q, int64_t Lpad, float* Yf,
-                    __nv_bfloat16* Yhi, __nv_bfloat16* Ylo, int* err, cudaStream_t stream) {
-  if (Yhi && Ylo && !Yf && err) {
-    const int rc = launch_temporal_split_tc(X, W, C, L, P, nt, Q, Lpad, Yhi, Ylo, err, stream);
-    if (rc == KS_OK) return zero_q_padding(C, P, Q, Lpad, Yf, Yhi, Ylo, stream);
-    if (rc != KS_ERR_UNSUPPORTED) return rc;
-  }
+static int launch_temporal_simt(const float* X, const float* W, int64_t C, int64_t L,
+                                int64_t P, int64_t nt, int64_t Q, int64_t Lpad, float* Yf,
+                                __nv_bfloat16* Yhi, __nv_bfloat16* Ylo, float* YT,
+                                int64_t ldyt, cudaStream_t stream) {
   const size_t smem = temporal_smem((int)nt, (int)P);
   const int tiles_t = (int)(Lpad / kTT);
   const long long n_tiles = (long long)tiles_t * ((C + kCG - 1) / kCG);
@@ -405,7 +414,7 @@ int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
     ks_temporal_kernel<PPV><<<grid, kTemporalThreads, smem, stream>>>(                     \
         X, W, (int)C, (int)L, (int)nt,                                                     \
                                                          (int)Q, tiles_t, (int)n_tiles,    \
-                                                         Yf, Yhi, Ylo);                    \
+                                                         Yf, Yhi, Ylo, YT, ldyt);          \
     break;                                                                                 \
   }
   switch (P) {
@@ -422,6 +431,29 @@ int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
   }
 #undef KS_TEMPORAL_CASE
   KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
+int launch_temporal_rows(const float* X, const float* W, int64_t C, int64_t L, int64_t P,
+                         int64_t nt, int64_t Lpad, float* YT, int64_t ldyt,
+                         cudaStream_t stream) {
+  if (Lpad % kTT || ldyt < Lpad || ldyt % 4 || (reinterpret_cast<uintptr_t>(YT) & 15))
+    return fail(KS_ERR_ARG, "temporal rows: Lpad % 128, ldyt >= Lpad, 16-byte rows");
+  return launch_temporal_simt(X, W, C, L, P, nt, round_up(round_up(C, kCG) * P, 64), Lpad,
+                              nullptr, nullptr, nullptr, YT, ldyt, stream);
+}
+
+int launch_temporal(const float* X, const float* W, int64_t C, int64_t L,
+                    int64_t P, int64_t nt, int64_t Q, int64_t Lpad, float* Yf,
+                    __nv_bfloat16* Yhi, __nv_bfloat16* Ylo, int* err, cudaStream_t stream) {
+  if (Yhi && Ylo && !Yf && err) {
+    const int rc = launch_temporal_split_tc(X, W, C, L, P, nt, Q, Lpad, Yhi, Ylo, err, stream);
+    if (rc == KS_OK) return zero_q_padding(C, P, Q, Lpad, Yf, Yhi, Ylo, stream);
+    if (rc != KS_ERR_UNSUPPORTED) return rc;
+  }
+  const int rc = launch_temporal_simt(X, W, C, L, P, nt, Q, Lpad, Yf, Yhi, Ylo, nullptr, 0,
+                                      stream);
+  if (rc) return rc;
   return zero_q_padding(C, P, Q, Lpad, Yf, Yhi, Ylo, stream);
 }
 

@@ -43,6 +43,11 @@ int launch_reorder_templates(const float* U, int64_t K, int64_t P, int64_t C, in
 int launch_temporal(const float* X, const float* W, int64_t C, int64_t L, int64_t P,
                     int64_t nt, int64_t Q, int64_t Lpad, float* Yf, __nv_bfloat16* Yhi,
                     __nv_bfloat16* Ylo, int* err, cudaStream_t stream);
+// FP32 temporal projection with rows (channel, component) and samples
+// contiguous: YT[(c * P + p) * ldyt + tau], tau < Lpad (a multiple of 128).
+int launch_temporal_rows(const float* X, const float* W, int64_t C, int64_t L, int64_t P,
+                         int64_t nt, int64_t Lpad, float* YT, int64_t ldyt,
+                         cudaStream_t stream);
 // Split-BF16 temporal projection on tcgen05 (temporal_tc.cu); KS_ERR_UNSUPPORTED
 // (nothing launched) for shapes it does not cover (odd P, P > 8, nt > 121).
 int launch_temporal_split_tc(const float* X, const float* W, int64_t C, int64_t L, int64_t P,
