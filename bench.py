@@ -56,7 +56,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batches", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="np1", choices=["np1", "uneven", "adjoint", "stream"],
+    p.add_argument("--workload", default="np1",
+                   choices=["np1", "uneven", "adjoint", "stream", "detect"],
                    help="np1: C=384/K=600, 20 equal batches (default); uneven: three "
                         "recordings, 200 batches of uneven length, batched launches; "
                         "adjoint: reconstruction loss + hand-written adjoint on one "
@@ -333,6 +334,72 @@ def adjoint_main(args, dev, rank, world):
     if rank == 0:
         print(json.dumps(line), flush=True)
 
+DETECT = ("universal-template detection (spikedetect.template_match + run's y and features): "
+          "C=384 (NP1-like, 1532 template positions x 5 sizes x 6 waveforms, 10 nearest "
+          "channels, 100 nearest positions), batches of 60000 samples (+2*61 pad) of the "
+          "C=384/K=600 synthetic recording, Th_universal=9, nt0min=20")
+
+
+def detect_main(args, dev, rank, world):
+    """Universal-template detection per batch, X resident; CPU oracle beside it."""
+    from kilosort_b200 import spikedetect, synth
+    rec = synth.config_recording(2, n_batches=3)
+    rng = np.random.default_rng(1006)
+    wave = synth._waveforms(rng, 6, NT, 20)
+    wTEMP = torch.from_numpy((wave / np.linalg.norm(wave, axis=1, keepdims=True)).astype(np.float32))
+    settings = dict(nearest_chans=10, nearest_templates=100, min_template_size=10,
+                    template_sizes=5, dmin=None, dminx=32, n_templates=6, n_pcs=6, nt0min=20)
+    ops = dict(settings=settings, xc=rec.xc.astype(np.float32), yc=rec.yc.astype(np.float32),
+               kcoords=np.zeros(rec.n_chan, np.float32), nt=NT, batch_size=NT_BATCH, fs=30000.0,
+               Th_universal=9.0, max_channel_distance=32.0, wTEMP=wTEMP,
+               wPCA=torch.from_numpy(rec.wPCA))
+    iC, iC2, weigh = spikedetect.geometry(ops, device=dev)
+    det = spikedetect.Detector(ops, iC, iC2, weigh, dev)
+    Xs = [torch.from_numpy(np.ascontiguousarray(rec.batch(b))).to(dev) for b in range(3)]
+    C, L = Xs[0].shape
+    for i in range(max(3, args.warmup)):
+        det(Xs[i % 3])
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev.index or 0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nsp = 0
+    sampler.__enter__()
+    e0.record()
+    for i in range(args.steps):
+        nsp += len(det(Xs[i % 3])[0])      # each call reads its count back (a sync)
+    e1.record()
+    torch.cuda.synchronize()
+    sampler.__exit__()
+    ms = e0.elapsed_time(e1) / args.steps
+    samples = C * (L - 2 * NT)
+    Nfilt = iC.shape[1]
+    line = {
+        "metric": "channel-samples/s", "value": samples * world / (ms * 1e-3),
+        "unit": "channel-samples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": DETECT, "positions": Nfilt,
+                   "l2": "3 batches of 92 MB rotated; the 554 MB convolution does not fit L2",
+                   "parallelism": f"replicas x{world}"},
+        "spikes_per_step": nsp / args.steps,
+        # FP32 work: the convolution 2*C*nk*nt*L, the sums 2*Nfilt*L*sizes*nk*nC
+        "gflop_per_step": (2 * C * 6 * NT * L + 2 * Nfilt * L * 5 * 6 * 10) / 1e9,
+        "clocks": sampler.summary(),
+        # memset, conv, scores, peaks, count, scan, emit, gather, features, finish
+        "gpu_launches": 9,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import detect as od
+        Xc = Xs[0][:, :15000 + 2 * NT].cpu()
+        t0 = time.perf_counter()
+        od.template_match(Xc, wTEMP, iC.cpu(), iC2.cpu(), weigh.cpu(), NT, 20, 9.0)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": C * 15000 / dt, "unit": "channel-samples/s",
+                                "cores": torch.get_num_threads(), "kind": "port",
+                                "sample": "template_match on one 15000-sample stretch (C=384)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
 STREAM = ("long dense recording, shortened: C=384 (NP1-like), K=2000 templates (amplitudes "
           "5-40 sd, 1-30 Hz), {nb} batches of 60000 samples streamed from page-locked host "
           "int16 (channel-mixed, scale 200) through the GPU batch filter (mean, CAR median, "
@@ -430,9 +497,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
 
-    if args.workload in ("uneven", "adjoint", "stream"):
-        {"uneven": uneven_main, "adjoint": adjoint_main,
-         "stream": stream_main}[args.workload](args, dev, rank, world)
+    if args.workload in ("uneven", "adjoint", "stream", "detect"):
+        {"uneven": uneven_main, "adjoint": adjoint_main, "stream": stream_main,
+         "detect": detect_main}[args.workload](args, dev, rank, world)
         if world > 1:
             dist.destroy_process_group()
         return

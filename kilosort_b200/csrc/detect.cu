@@ -10,8 +10,11 @@
 //   y = sum_j relu(adist_j)/sum relu(adist) * yc[iC[j, f]];
 //   tF[s, j, p] = sum_u X[iC[j, f], t - nt/2 + u] * wPCA[p, u]
 //
-// Kernels: ks_detect_scores_kernel (one thread per (f, t), warps over 32
-// consecutive samples, the (s, k) sums in registers; A is never stored),
+// Kernels: ks_detect_scores_tiled_kernel (a block per tile of 32 positions,
+// persistent over 32-sample time tiles: the union of the positions' nearest
+// channels is staged, double-buffered by cp.async, the (s, k) sums of one
+// position over 32 samples per warp in registers; A is never stored;
+// ks_detect_scores_kernel is the form for more than 8192 channels),
 // ks_detect_peaks_kernel (a block per (f, 256-sample tile): neighbour maximum
 // over the tile and its +-nt0 halo in shared memory, sliding maximum, peak
 // bits by warp ballot), count / scan / emit in (f, t) order, and one gather
@@ -93,6 +96,210 @@ ks_detect_scores_kernel(const float* __restrict__ BT, long long ldb, int nk, int
   imaxs[(long long)f * L + t] = (signed char)((1 + bidx) * sg);
 }
 
+// The same sums for a tile of kFT consecutive positions x kTT samples: the
+// block first collects the union of its positions' nearest channels (a
+// bitmap over channels, compacted in channel order), stages those channels'
+// convolution rows for its samples in shared memory, then each warp computes
+// one position over 32 consecutive samples per round.  A tile whose union
+// exceeds kMaxU channels reads its rows from global memory instead.
+constexpr int kFT = 32;          // positions per block
+constexpr int kTT = 32;          // samples per time tile
+constexpr int kMaxU = 48;        // staged channels
+constexpr int kMaxCBits = 8192;  // channels covered by the bitmap
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait1() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait0() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// Persistent over time: block (position tile, y) takes the time tiles y,
+// y + gridDim.y, ...; the union of its positions' channels and their weights
+// are set up once, and the channels' convolution rows of the next time tile
+// are copied (cp.async, 16-byte pieces) while the current one is summed.
+template <int NS, int NK>
+__global__ void __launch_bounds__(256)
+ks_detect_scores_tiled_kernel(const float* __restrict__ BT, long long ldb, int nk_rt, int C,
+                              const long long* __restrict__ iC, int nC,
+                              const float* __restrict__ weigh, int ns_rt, int Nfilt, int L,
+                              int n_ttiles, float* __restrict__ As,
+                              signed char* __restrict__ imaxs, int* err) {
+  // NS, NK: compile-time bounds of the sizes and waveforms; ns_rt, nk_rt the
+  // actual counts (equal to the bounds in the specialised instantiation)
+  extern __shared__ __align__(16) float sm[];
+  float* sB = sm;                                                // [2][kMaxU][NK][kTT]
+  float* sw = sB + 2 * kMaxU * NK * kTT;                         // [kFT][nC][NS]
+  unsigned* bitmap = reinterpret_cast<unsigned*>(sw + kFT * NS * nC);   // [kMaxCBits / 32]
+  int* wpre = reinterpret_cast<int*>(bitmap + kMaxCBits / 32);   // [kMaxCBits / 32]
+  int* ulist = wpre + kMaxCBits / 32;                            // [kMaxU]
+  int* cidx = ulist + kMaxU;                                     // [kMaxNC][kFT] channel
+  int* loc = cidx + kMaxNC * kFT;                                // [kMaxNC][kFT] union slot
+  __shared__ int nU;
+  const int ns = NS == kMaxNS ? ns_rt : NS;
+  const int nk = NK == kMaxNK ? nk_rt : NK;
+  const int f0 = blockIdx.x * kFT;
+  const int nwc = (C + 31) >> 5;
+  for (int w = threadIdx.x; w < nwc; w += blockDim.x) bitmap[w] = 0u;
+  __syncthreads();
+  for (int e = threadIdx.x; e < nC * kFT; e += blockDim.x) {
+    const int j = e / kFT, fl = e % kFT;
+    const int f = f0 + fl;
+    int c = 0;
+    if (f < Nfilt) {
+      const long long cc = iC[(long long)j * Nfilt + f];
+      if (cc < 0 || cc >= C) atomicCAS(err, 0, KS_ERR_ARG);   // channel 0 stands in
+      else c = (int)cc;
+    }
+    cidx[e] = c;
+    atomicOr(bitmap + (c >> 5), 1u << (c & 31));
+  }
+  // weights [fl][j][q] (zero for missing sizes and positions)
+  for (int e = threadIdx.x; e < kFT * nC * NS; e += blockDim.x) {
+    const int fl = e / (nC * NS), r = e - fl * nC * NS, j = r / NS, q = r % NS;
+    const int f = f0 + fl;
+    sw[e] = (f < Nfilt && q < ns) ? weigh[((long long)q * nC + j) * Nfilt + f] : 0.f;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    // exclusive prefix of the bitmap words' population counts
+    int run = 0;
+    for (int w0 = 0; w0 < nwc; w0 += 32) {
+      const int w = w0 + threadIdx.x;
+      const int cnt = w < nwc ? __popc(bitmap[w]) : 0;
+      int incl = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((int)threadIdx.x >= o) incl += v;
+      }
+      if (w < nwc) wpre[w] = run + incl - cnt;
+      run += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (threadIdx.x == 0) nU = run;
+  }
+  __syncthreads();
+  const bool staged = nU <= kMaxU;
+  for (int e = threadIdx.x; e < nC * kFT; e += blockDim.x) {
+    const int c = cidx[e];
+    loc[e] = wpre[c >> 5] + __popc(bitmap[c >> 5] & ((1u << (c & 31)) - 1u));
+    if (staged) ulist[loc[e]] = c;
+  }
+  __syncthreads();
+  // rows (u, k) of a time tile: kTT floats = kTT/4 16-byte pieces each
+  auto fetch = [&](int tt, int buf) {
+    if (staged) {
+      const int n = nU * nk * (kTT / 4);
+      float* dst = sB + buf * kMaxU * NK * kTT;
+      for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const int row = e / (kTT / 4), piece = e % (kTT / 4);
+        const int u = row / nk, k = row % nk;
+        cp_async16(dst + (u * NK + k) * kTT + piece * 4,
+                   BT + ((long long)ulist[u] * nk + k) * ldb + (long long)tt * kTT + piece * 4);
+      }
+    }
+    cp_async_commit();
+  };
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int buf = 0;
+  if ((int)blockIdx.y < n_ttiles) fetch(blockIdx.y, 0);
+  for (int tt = blockIdx.y; tt < n_ttiles; tt += gridDim.y) {
+    const int next = tt + gridDim.y;
+    if (next < n_ttiles) fetch(next, buf ^ 1);
+    else cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    const float* cur = sB + buf * kMaxU * NK * kTT;
+    const int t = tt * kTT + lane;
+    for (int fl = warp; fl < kFT; fl += 8) {
+      const int f = f0 + fl;
+      float a[NS][NK];
+#pragma unroll
+      for (int q = 0; q < NS; ++q)
+#pragma unroll
+        for (int k = 0; k < NK; ++k) a[q][k] = 0.f;
+      for (int j = 0; j < nC; ++j) {
+        float bk[NK];
+        if (staged) {
+          const float* b = cur + (loc[j * kFT + fl] * NK) * kTT + lane;
+#pragma unroll
+          for (int k = 0; k < NK; ++k) bk[k] = b[k * kTT];
+        } else {
+          const float* b = BT + (long long)cidx[j * kFT + fl] * nk * ldb + t;
+#pragma unroll
+          for (int k = 0; k < NK; ++k) bk[k] = k < nk ? __ldg(b + (long long)k * ldb) : 0.f;
+        }
+        const float* w = sw + (fl * nC + j) * NS;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+          const float wq = w[q];
+#pragma unroll
+          for (int k = 0; k < NK; ++k) a[q][k] = fmaf(wq, bk[k], a[q][k]);
+        }
+      }
+      // largest magnitude, first index in (size, waveform) order
+      float best = -1.f, bval = 0.f;
+      int bidx = 0;
+#pragma unroll
+      for (int q = 0; q < NS; ++q)
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+          if (q < ns && k < nk) {
+            const float m = fabsf(a[q][k]);
+            if (m > best) {
+              best = m;
+              bval = a[q][k];
+              bidx = q * nk + k;
+            }
+          }
+      if (f < Nfilt && t < L) {
+        const int sg = bval > 0.f ? 1 : (bval < 0.f ? -1 : 0);
+        As[(long long)f * L + t] = best;
+        imaxs[(long long)f * L + t] = (signed char)((1 + bidx) * sg);
+      }
+    }
+    __syncthreads();          // the buffer is read: the next fetch may reuse it
+    buf ^= 1;
+  }
+  cp_async_wait0();
+}
+
+size_t scores_tiled_smem(int NK, int NS, int nC) {
+  return sizeof(unsigned) * (kMaxCBits / 32) * 2 + sizeof(int) * (kMaxU + 2 * kMaxNC * kFT) +
+         sizeof(float) * ((size_t)kFT * NS * nC + 2 * (size_t)kMaxU * NK * kTT);
+}
+
+template <int NS, int NK>
+int launch_scores_tiled(const float* BT, long long ldb, int nk, int C, const long long* iC,
+                        int nC, const float* weigh, int ns, int Nfilt, int L, float* As,
+                        signed char* ims, int* err, cudaStream_t s) {
+  const size_t smem = scores_tiled_smem(NK, NS, nC);
+  KS_CUDA(cudaFuncSetAttribute(ks_detect_scores_tiled_kernel<NS, NK>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ks::DeviceInfo dev;
+  int rc = ks::device_info(&dev);
+  if (rc) return rc;
+  int occ = 0;
+  KS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ks_detect_scores_tiled_kernel<NS, NK>,
+                                                        256, smem));
+  const int ftiles = (Nfilt + kFT - 1) / kFT;
+  const int n_ttiles = (L + kTT - 1) / kTT;
+  // about one wave of resident blocks, each walking its share of the time tiles
+  const int gy = std::max(1, std::min(n_ttiles, std::max(occ, 1) * dev.sm_count / ftiles));
+  const dim3 grid((unsigned)ftiles, (unsigned)gy);
+  ks_detect_scores_tiled_kernel<NS, NK><<<grid, 256, smem, s>>>(BT, ldb, nk, C, iC, nC, weigh,
+                                                                ns, Nfilt, L, n_ttiles, As, ims,
+                                                                err);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
 // Neighbour maximum, +-nt0 max-pool, peak test; one block per (f, tile).
 __global__ void __launch_bounds__(kTile)
 ks_detect_peaks_kernel(const float* __restrict__ As, const long long* __restrict__ iC2,
@@ -113,7 +320,17 @@ ks_detect_peaks_kernel(const float* __restrict__ As, const long long* __restrict
     const int t = t0 - nt0 + u;
     float m = 0.f;                                 // edges and the halo outside the batch
     if (t >= nt && t < L - nt) {
-      for (int j = 0; j < nC2; ++j) m = fmaxf(m, As[(long long)snb[j] * L + t]);
+      // four independent partial maxima keep several loads in flight
+      float m1 = 0.f, m2 = 0.f, m3 = 0.f;
+      int j = 0;
+      for (; j + 4 <= nC2; j += 4) {
+        m = fmaxf(m, As[(long long)snb[j] * L + t]);
+        m1 = fmaxf(m1, As[(long long)snb[j + 1] * L + t]);
+        m2 = fmaxf(m2, As[(long long)snb[j + 2] * L + t]);
+        m3 = fmaxf(m3, As[(long long)snb[j + 3] * L + t]);
+      }
+      for (; j < nC2; ++j) m = fmaxf(m, As[(long long)snb[j] * L + t]);
+      m = fmaxf(fmaxf(m, m1), fmaxf(m2, m3));
     }
     amax[u] = m;
   }
@@ -365,7 +582,16 @@ extern "C" KS_API int ks_detect(const float* X, int64_t C, int64_t L, const floa
   int rc = launch_temporal_rows(X, wTEMP, C, L, nk, nt, d.Lpad, BT, d.Lpad, s);
   if (rc) return rc;
   // 2. scores over sizes and waveforms
-  {
+  if (C <= kMaxCBits) {
+    // the reference's defaults (5 sizes, 6 waveforms) have their own instantiation
+    rc = (nsizes == 5 && nk == 6)
+             ? launch_scores_tiled<5, 6>(BT, d.Lpad, (int)nk, (int)C, iCl, (int)nC, weigh,
+                                         (int)nsizes, (int)Nfilt, (int)L, As, ims, err, s)
+             : launch_scores_tiled<kMaxNS, kMaxNK>(BT, d.Lpad, (int)nk, (int)C, iCl, (int)nC,
+                                                   weigh, (int)nsizes, (int)Nfilt, (int)L, As,
+                                                   ims, err, s);
+    if (rc) return rc;
+  } else {
     const dim3 grid((unsigned)Nfilt, (unsigned)((L + kTile - 1) / kTile));
     ks_detect_scores_kernel<<<grid, kTile, 0, s>>>(BT, d.Lpad, (int)nk, (int)C, iCl, (int)nC, weigh,
                                                    (int)nsizes, (int)Nfilt, (int)L, As, ims, err);
