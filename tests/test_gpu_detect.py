@@ -99,3 +99,13 @@ def test_bad_channel_index_is_reported(cuda_device):
     X = torch.from_numpy(np.ascontiguousarray(rec.batch(0))).to(DEV)
     with pytest.raises(_lib.KilosortB200Error):
         sd.Detector(ops, iC, iC2, weigh, DEV)(X)
+
+
+def test_zero_batch_has_no_spikes(cuda_device):
+    rec = synth.make_recording(**ast.literal_eval(str(G["seed_kwargs"])))
+    ops = _ops(rec)
+    iC, iC2, weigh = sd.geometry(ops, device=DEV)
+    X = torch.zeros((rec.n_chan, 3122), device=DEV)
+    xy, imax, amp, adist, yct, tF = sd.Detector(ops, iC, iC2, weigh, DEV)(X)
+    assert len(xy) == len(imax) == len(amp) == len(yct) == len(tF) == 0
+    assert adist.shape == (iC.shape[0], 0)

@@ -83,3 +83,12 @@ def test_similarity_cfg2_templates(cuda_device):
     assert np.abs(sim - ref).max() <= 1e-5 * np.abs(ref).max()
     # each template is most similar to itself (unit norm: about 1 at lag 0)
     assert np.all(np.abs(np.diag(sim) - 1) < 1e-3)
+
+
+def test_similarity_single_template(cuda_device):
+    rec = synth.make_recording(8301, n_chan=16, n_templates=1, batch_lengths=[3000])
+    Wall = torch.from_numpy(rec.U).transpose(1, 2).contiguous()
+    sim = postprocess.template_similarity(Wall.to(DEV), torch.from_numpy(rec.wPCA).to(DEV),
+                                          rec.nt)
+    ref = op.similarity(Wall, torch.from_numpy(rec.wPCA), rec.nt)
+    assert sim.shape == (1, 1) and abs(sim[0, 0] - ref[0, 0]) <= 1e-5

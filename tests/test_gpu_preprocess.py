@@ -117,3 +117,15 @@ def test_stream_with_preprocessing_equals_per_batch(cuda_device):
         ref_k.append(st[:, 1])
     np.testing.assert_array_equal(times, np.concatenate(ref_t))
     np.testing.assert_array_equal(templ, np.concatenate(ref_k))
+
+
+def test_single_channel_and_odd_length(cuda_device):
+    """C = 1 (no CAR: the median of one channel is itself), odd batch length
+    with the high-pass, against the oracle in float64."""
+    raw = synth.raw_batch(7103, 3, 1501)
+    hp = op.highpass_filter()
+    p = Preprocessor(3, 1501, chan_map=np.array([2]), hp_filter=hp, do_CAR=False, device=DEV)
+    X = p(torch.from_numpy(raw).to(DEV)).cpu().numpy()
+    ref = op.filter_batch(torch.from_numpy(raw.T.astype(np.float64)), chan_map=torch.tensor([2]),
+                          do_car=False, hp=hp.double()).numpy()
+    assert np.abs(X - ref).max() <= 1e-5 * np.abs(ref).max()
