@@ -11,7 +11,8 @@ captured graph: grouped tensor-core contraction, one cooperative peel launch
 split into autotuned teams, one residual launch).  `value` is channel-samples/s
 of the batched split form.  `e2e` runs that form from pinned host memory, with
 the host->device copy of X and the device->host copy of the spikes inside the
-timed region.
+timed region, through the pipelined front end (batched.HostPipeline: groups
+of KS_BENCH_E2E_GROUP = 5 batches, copies and read-back beside the matching).
 
     python bench.py --workload uneven     # three recordings, 200 uneven batches
     python bench.py --workload adjoint    # reconstruction loss + adjoint
@@ -37,6 +38,7 @@ import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
 NT_BATCH = 60000
+E2E_GROUP = int(os.environ.get("KS_BENCH_E2E_GROUP", "5"))   # batches per pipelined group
 NT = 61
 N_PCS = 6
 TH = 8.0
@@ -615,14 +617,18 @@ def main():
             d2h[0] += st_h.numel() * 8 + a_h.numel() * 4 + t_h.numel() * 4
         spikes.append(n)
 
+    pipe = None
+    if matcher is not None:
+        from kilosort_b200.batched import HostPipeline
+        # groups of E2E_GROUP batches: the copies of one group and the read-back
+        # of the previous run beside the matching of the current one
+        pipe = HostPipeline([mrec], [(L, 0)] * len(Xh), "bf16x3",
+                            teams=min(teams, E2E_GROUP), group=E2E_GROUP)
+
     def e2e_batched(form, spikes):
-        for dst, Xhost in zip(matcher.X, Xh):
-            dst.copy_(Xhost, non_blocking=True)
-        matcher.launch()
         n = 0
         d2h[0] = 0
-        for st, amps, th, _ in matcher.results():
-            st_h, a_h, t_h = st.cpu(), amps.cpu(), th.cpu()
+        for st_h, a_h, t_h in pipe.run(Xh):
             n += len(st_h)
             d2h[0] += st_h.numel() * 8 + a_h.numel() * 4 + t_h.numel() * 4
         spikes.append(n)

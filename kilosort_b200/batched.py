@@ -15,6 +15,8 @@ residual launch.  Each batch gets exactly what ``run_matching`` returns for it.
 * ``autotune_teams`` times candidate team counts on the device and caches the
                      fastest per workload signature; ``autotune_schedule``
                      also picks the number of pipelined groups
+* ``HostPipeline``   batches in host memory: two captured matchers alternate
+                     so transfers and read-back overlap the matching
 """
 from __future__ import annotations
 
@@ -357,3 +359,94 @@ class BatchedMatcher:
                 dst.copy_(src, non_blocking=True)
         self.launch()
         return self.results()
+
+
+class HostPipeline:
+    """Match batches held in host memory, transfers overlapped with matching.
+
+    The batches are split into consecutive groups of ``group``; two captured
+    ``BatchedMatcher`` graphs alternate, so while group g is matched the
+    copies of group g+1 into the other matcher's inputs (copy stream) and
+    the read-back of group g-1's spikes (read-back stream) proceed.  Host
+    batches should be page-locked (``pin_memory``) for the copies to be
+    asynchronous.  ``run`` returns per batch ``(st, amps, th_amps)`` on the
+    host, in input order, equal to what ``run_matching`` returns for that
+    batch.
+    """
+
+    def __init__(self, recs: Sequence[Recording], lengths: Sequence[Tuple[int, int]],
+                 projection: str = "bf16x3", teams: Optional[int] = 0, group: int = 5):
+        self.recs = list(recs)
+        self.lengths = [(int(L), int(r)) for L, r in lengths]
+        self.projection = projection
+        self.teams = teams
+        self.group = max(1, int(group))
+        self.device = self.recs[0].U.device
+        n = len(self.lengths)
+        self.groups = [list(range(g0, min(g0 + self.group, n))) for g0 in range(0, n, self.group)]
+        self._matchers = {}
+        self.copy = torch.cuda.Stream(self.device)
+        self.readback = torch.cuda.Stream(self.device)
+        self.copied = [torch.cuda.Event() for _ in range(2)]
+        self.done = [torch.cuda.Event() for _ in range(2)]
+
+    def _matcher(self, g: int) -> BatchedMatcher:
+        shape = tuple(self.lengths[b] for b in self.groups[g])
+        key = (g % 2, shape)
+        if key not in self._matchers:
+            self._matchers[key] = BatchedMatcher(self.recs, list(shape), self.projection,
+                                                 teams=self.teams, graph=True)
+        return self._matchers[key]
+
+    def run(self, Xh: Sequence[torch.Tensor]):
+        if len(Xh) != len(self.lengths):
+            raise ValueError(f"expected {len(self.lengths)} batches, got {len(Xh)}")
+        ms = [self._matcher(g) for g in range(len(self.groups))]
+        cur = torch.cuda.current_stream(self.device)
+        out = [None] * len(Xh)
+
+        def enqueue_copy(g):
+            m = ms[g]
+            with torch.cuda.stream(self.copy):
+                # the matcher's previous launch has finished reading its inputs
+                self.copy.wait_event(self.done[g % 2])
+                for i, b in enumerate(self.groups[g]):
+                    m.X[i].copy_(Xh[b], non_blocking=True)
+                self.copied[g % 2].record(self.copy)
+
+        def collect(g):
+            m = ms[g]
+            with torch.cuda.stream(self.readback):
+                self.readback.wait_event(self.done[g % 2])
+                info = m.info.to("cpu", non_blocking=True)
+                self.readback.synchronize()
+                host = []
+                for i, b in enumerate(self.groups[g]):
+                    n, status, _, need = (int(v) for v in info[i].tolist())
+                    if status == _lib.KS_ERR_OVERFLOW:
+                        raise RuntimeError(f"HostPipeline: batch {b} needs {need} spikes, above "
+                                           f"the capacity {m.outs[i].st.shape[0]}")
+                    if status != _lib.KS_OK:
+                        raise _lib.KilosortB200Error(status, f"HostPipeline: batch {b}: "
+                                                     f"device status {status}")
+                    o = m.outs[i]
+                    host.append((b, o.st[:n].to("cpu", non_blocking=True),
+                                 o.amps[:n].to("cpu", non_blocking=True),
+                                 o.th_amps[:n].to("cpu", non_blocking=True)))
+                self.readback.synchronize()
+            for b, st, amps, th in host:
+                out[b] = (st, amps, th)
+
+        if self.groups:
+            enqueue_copy(0)
+        for g in range(len(self.groups)):
+            if g + 1 < len(self.groups):
+                enqueue_copy(g + 1)
+            cur.wait_event(self.copied[g % 2])
+            ms[g].launch()
+            self.done[g % 2].record(cur)
+            if g >= 1:
+                collect(g - 1)
+        if self.groups:
+            collect(len(self.groups) - 1)
+        return out

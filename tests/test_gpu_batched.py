@@ -144,3 +144,22 @@ def test_in_place_residual(cuda_device):
     res = m.run([X for X, _ in items])
     _assert_same(res, ref)
     assert all(res[i][3].data_ptr() == m.X[i].data_ptr() for i in range(len(items)))
+
+
+def test_host_pipeline_equals_per_batch(cuda_device):
+    """Batches in pinned host memory through the pipelined front end: groups
+    of 3 alternate between two captured matchers (the last group is short)."""
+    from kilosort_b200.batched import HostPipeline
+    recs = _recordings()
+    setup = _setup(recs)
+    items = _items(recs)
+    ref = _reference(setup, items, "bf16x3")
+    pipe = HostPipeline([s[3] for s in setup], [(X.shape[1], r) for X, r in items], "bf16x3",
+                        teams=2, group=3)
+    host = [X.cpu().pin_memory() for X, _ in items]
+    for _ in range(2):                       # a second run replays the graphs
+        res = pipe.run(host)
+        for (st, amps, th), (st_r, amps_r, th_r, _) in zip(res, ref):
+            assert torch.equal(st, st_r.cpu())
+            assert torch.equal(amps, amps_r.cpu())
+            assert torch.equal(th, th_r.cpu())
