@@ -317,7 +317,13 @@ class BatchedMatcher:
         self._prepare()
         if self.graph_enabled:
             if self._graph is None:
-                self._enqueue()                    # warm-up: first-use set-up out of capture
+                # warm-up: first-use set-up out of capture; a residual written
+                # in place overwrites the inputs, so they are put back after it
+                saved = [X.clone() for X, o in zip(self.X, self.outs) if o.Xres is X]
+                self._enqueue()
+                for X, s in zip((X for X, o in zip(self.X, self.outs) if o.Xres is X), saved):
+                    X.copy_(s)
+                del saved
                 torch.cuda.synchronize(self.device)
                 g = torch.cuda.CUDAGraph()
                 s = torch.cuda.Stream(self.device)

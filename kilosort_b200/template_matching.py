@@ -357,13 +357,71 @@ def _match_features(ops, W, iCCd, iU, Ucc):
     return match, features
 
 
-def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=None):
+class _BatchReader:
+    """Reads ``bfile.padded_batch_to_torch`` one batch ahead on a worker
+    thread, so the next batch's file read and host->device copy overlap the
+    current batch's matching.
+
+    On a CUDA device the read runs on the reader's own stream and is complete
+    when handed over (the stream is synchronised in the worker); the tensor is
+    then recorded on the consumer's stream so its memory is not reused while
+    that stream may still read it.
+    """
+
+    def __init__(self, bfile, order, ops, device=None, ahead=True):
+        self.bfile, self.order, self.ops = bfile, list(order), ops
+        self.device = torch.device(device) if device is not None else None
+        self.pool = None
+        self.next = None
+        if ahead and len(self.order) > 1:
+            from concurrent.futures import ThreadPoolExecutor
+            self.pool = ThreadPoolExecutor(1, thread_name_prefix="ks-batch-reader")
+            self.streams = {}
+            self.next = self.pool.submit(self._read, self.order[0])
+
+    def _read(self, ibatch):
+        dev = self.device
+        if self.pool is None or dev is None or dev.type != "cuda":
+            return self.bfile.padded_batch_to_torch(ibatch, self.ops)
+        if dev not in self.streams:
+            self.streams[dev] = torch.cuda.Stream(dev)
+        s = self.streams[dev]
+        with torch.cuda.device(dev), torch.cuda.stream(s):
+            X = self.bfile.padded_batch_to_torch(ibatch, self.ops)
+        s.synchronize()
+        return X
+
+    def get(self, pos):
+        """The batch ``order[pos]``; positions are taken in increasing order."""
+        if self.pool is None:
+            return self._read(self.order[pos])
+        X = self.next.result()
+        self.next = (self.pool.submit(self._read, self.order[pos + 1])
+                     if pos + 1 < len(self.order) else None)
+        if isinstance(X, torch.Tensor) and X.is_cuda:
+            X.record_stream(torch.cuda.current_stream(X.device))
+        return X
+
+    def close(self):
+        if self.pool is not None:
+            if self.next is not None:
+                self.next.cancel()
+            self.pool.shutdown(wait=True)
+            self.pool = None
+
+
+def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=None,
+                    read_ahead=True):
     """Rows ``[N, 3]`` (time, template, th_amp; float64 numpy) and features
     ``[N, nC, P]`` (CPU tensor) of the given batches, in batch order, before
     the final sort -- the loop body of kilosort/template_matching.py:79-110.
 
     ``match(X, U, ctc, device)`` returns ``(st, amps, th_amps, Xres)`` and
     ``features(Xres, st, amps)`` the ``[N, nC, P]`` features of one batch.
+    With ``read_ahead`` the next batch is read while the current one is
+    matched (the same batches in the same order).  Rows are gathered per
+    batch and joined once at the end (the reference grows preallocated
+    buffers of 10**6 rows; the returned rows are the same).
     """
     try:
         from tqdm import tqdm
@@ -371,18 +429,18 @@ def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=N
         tqdm = None
     nt = ops["nt"]
     nC = ops["settings"]["nearest_chans"]
-    st = np.zeros((10 ** 6, 3), "float64")
-    tF = torch.zeros((10 ** 6, nC, ops["settings"]["n_pcs"]))
-    k = 0
+    sts, tFs = [], []
     prog = tqdm(batches, miniters=200 if progress_bar else None,
                 mininterval=60 if progress_bar else None) if tqdm else batches
     ibatch = -1
+    reader = _BatchReader(bfile, [int(b) for b in batches], ops, device=U.device,
+                          ahead=read_ahead)
     try:
-        for ibatch in prog:
+        for pos, ibatch in enumerate(prog):
             ibatch = int(ibatch)
             if ibatch % 100 == 0 and torch.cuda.is_available():
                 logger.debug(f"Batch {ibatch}: {torch.cuda.memory_allocated() / 2**30:.2f} GiB allocated")
-            X = bfile.padded_batch_to_torch(ibatch, ops)
+            X = reader.get(pos)
             stt, amps, th_amps, Xres = match(X, U, ctc, X.device)
             xfeat = features(Xres, stt, amps)
             if ibatch == 0:
@@ -391,23 +449,24 @@ def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=N
                 xfeat = xfeat[~neg]
                 amps = amps[~neg, :]
                 th_amps = th_amps[~neg, :]
-            nsp = len(stt)
-            while k + nsp > st.shape[0]:
-                st = np.concatenate((st, np.zeros_like(st)), 0)
-                tF = torch.cat((tF, torch.zeros_like(tF)), 0)
             t_shift = ibatch * bfile.batch_downsampling * (ops["batch_size"])
             stt = stt.double()
-            st[k:k + nsp, 0] = ((stt[:, 0] - nt) + t_shift).cpu().numpy() - nt // 2 + ops["nt0min"]
-            st[k:k + nsp, 1] = stt[:, 1].cpu().numpy()
-            st[k:k + nsp, 2] = th_amps.cpu().numpy().squeeze(-1)
-            tF[k:k + nsp] = xfeat.cpu()
-            k += nsp
+            rows = np.empty((len(stt), 3), "float64")
+            rows[:, 0] = ((stt[:, 0] - nt) + t_shift).cpu().numpy() - nt // 2 + ops["nt0min"]
+            rows[:, 1] = stt[:, 1].cpu().numpy()
+            rows[:, 2] = th_amps.cpu().numpy().squeeze(-1)
+            sts.append(rows)
+            tFs.append(xfeat.cpu())
             if progress_bar is not None:
                 progress_bar.emit(int((ibatch + 1) / bfile.n_batches * 100))
     except Exception:
         logger.exception(f"Error in kilosort_b200.extract on batch {ibatch}")
         raise
-    return st[:k], tF[:k]
+    finally:
+        reader.close()
+    st = np.concatenate(sts) if sts else np.zeros((0, 3), "float64")
+    tF = torch.cat(tFs) if tFs else torch.zeros((0, nC, ops["settings"]["n_pcs"]))
+    return st, tF
 
 
 def sort_spikes(st, tF):

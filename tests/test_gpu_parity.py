@@ -264,3 +264,27 @@ def test_transposed_ctc_cache_follows_the_tensor(cuda_device):
         st_r, amps_r, _, _ = om.run_matching(ops, X, U, ctc.cpu())
         np.testing.assert_array_equal(st.cpu().numpy(), st_r.numpy())
         del ctc                               # its storage goes back to the allocator
+
+
+def test_extract_read_ahead_equals_in_order_reads(cuda_device):
+    """extract reads the next batch on a worker thread and stream while the
+    current one is matched; the result equals reading each batch in turn."""
+    from kilosort_b200 import template_matching as tm
+    rec = synth.make_recording(2101, n_chan=32, probe="np1", n_templates=24,
+                               batch_lengths=[3000] * 5, rate_hz=(10.0, 30.0))
+    ops = dict(Th_learned=8.0, nt=61, max_peels=100, wPCA=torch.from_numpy(rec.wPCA).to(DEV),
+               nt0min=20, batch_size=3000, xc=rec.xc, yc=rec.yc,
+               settings=dict(nearest_chans=10, position_limit=100, n_pcs=6))
+    U = torch.from_numpy(rec.U).to(DEV)
+    st, tF, ops = kb.extract(ops, synth.SyntheticBinary(rec, device=DEV), U, device=DEV)
+    assert len(st) > 100
+    match, features = tm._match_features(ops, ops["wPCA"].contiguous(),
+                                         ops["iCC"].to(DEV).contiguous(), ops["iU"],
+                                         kb.prepare_extract(rec.xc, rec.yc, U, 10, 100,
+                                                            device=DEV)[3])
+    st1, tF1 = tm.extract_batches(ops, synth.SyntheticBinary(rec, device=DEV), np.arange(5), U,
+                                  kb.prepare_matching(ops, U), match, features,
+                                  read_ahead=False)
+    st1, tF1 = tm.sort_spikes(st1, tF1)
+    np.testing.assert_array_equal(st, st1)
+    assert torch.equal(tF, tF1)

@@ -167,3 +167,51 @@ def test_gradient_allreduce_equals_gradient_of_summed_loss(tmp_path):
                                    rtol=1e-12, atol=1e-9)
         np.testing.assert_allclose(np.load(tmp_path / f"dW{r}.npy"), Wd.grad.numpy(),
                                    rtol=1e-12, atol=1e-9)
+
+
+class _CountingSource:
+    """A batch source that records the order of reads and can fail on one."""
+
+    def __init__(self, n, fail_at=None):
+        self.n_batches, self.batch_downsampling = n, 1
+        self.reads, self.fail_at = [], fail_at
+
+    def padded_batch_to_torch(self, ibatch, ops=None):
+        self.reads.append(int(ibatch))
+        if ibatch == self.fail_at:
+            raise OSError(f"cannot read batch {ibatch}")
+        return torch.full((2, 5), float(ibatch))
+
+
+@pytest.mark.parametrize("ahead", [False, True])
+def test_batch_reader_order_and_errors(ahead):
+    from kilosort_b200.template_matching import _BatchReader
+    src = _CountingSource(6)
+    r = _BatchReader(src, [3, 4, 5], None, device="cpu", ahead=ahead)
+    assert [r.get(i)[0, 0].item() for i in range(3)] == [3.0, 4.0, 5.0]
+    r.close()
+    assert src.reads == [3, 4, 5]
+    src = _CountingSource(6, fail_at=1)
+    r = _BatchReader(src, range(4), None, device="cpu", ahead=ahead)
+    assert r.get(0)[0, 0].item() == 0.0
+    with pytest.raises(OSError, match="batch 1"):
+        r.get(1)
+    r.close()
+
+
+def test_extract_read_ahead_equals_reference_extract():
+    """extract_batches with and without the read-ahead reader give the
+    reference's own extract output (oracle matcher, CPU)."""
+    from kilosort_b200 import template_matching as tm
+    g, rec = _golden_case()
+    ops = _ops(rec)
+    _, match, features = _oracle_fns(rec, ops)
+    U = torch.from_numpy(rec.U)
+    ctc = om.prepare_matching(ops, U)
+    batches = np.arange(synth.SyntheticBinary(rec).n_batches, dtype=np.int64)
+    for ahead in (False, True):
+        st, tF = tm.extract_batches(ops, synth.SyntheticBinary(rec, device="cpu"), batches, U,
+                                    ctc, match, features, read_ahead=ahead)
+        st, tF = tm.sort_spikes(st, tF)
+        np.testing.assert_array_equal(st, g["st"])
+        np.testing.assert_array_equal(tF.numpy(), g["tF"])
