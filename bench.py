@@ -46,6 +46,9 @@ CFG = 2
 # DRAM bytes (read + write) of one peel_kernel launch on a C=384/K=600/60000-sample
 # batch, from the ncu capture summarised in profiles/peel_kernel_c384_k600.txt
 PEEL_TRAFFIC_BYTES = 8.678e9
+# DRAM bytes of one peel_multi_kernel launch over 20 such batches (20 teams, one
+# group), per batch, from profiles/peel_multi_kernel_c384_k600_20batches.txt
+PEEL_MULTI_TRAFFIC_BYTES_PER_BATCH = 182.941e9 / 20
 WORKLOAD = ("Neuropixels-scale matching: C=384 (NP1-like), K=600 templates, 20 batches x "
             "60000 samples (+2*61 pad), nt=61, n_pcs=6, Th_learned=8, max_peels=100")
 
@@ -70,6 +73,9 @@ def parse():
                    help="uneven workload: batches per batched call (one graph each)")
     p.add_argument("--group-stream", type=int, default=4,
                    help="stream workload: batches per batched call")
+    p.add_argument("--schedule", default=None,
+                   help="np1 workload: 'TEAMS,GROUPS' of the batched form instead of the "
+                        "autotuned schedule (for profiling a fixed launch)")
     return p.parse_args()
 
 
@@ -584,8 +590,11 @@ def main():
         from kilosort_b200.batched import BatchedMatcher, Recording, autotune_schedule
         mrec = Recording.from_ops(ops, U, ctc)
         items = [(X, 0) for X in Xs]
-        teams, groups = autotune_schedule([mrec], items, "bf16x3", teams=(5, 10, 20),
-                                          groups=(1, 2, 4, 5))
+        if args.schedule:
+            teams, groups = (int(v) for v in args.schedule.split(","))
+        else:
+            teams, groups = autotune_schedule([mrec], items, "bf16x3", teams=(5, 10, 20),
+                                              groups=(1, 2, 4, 5))
         matcher = BatchedMatcher([mrec], [(L, 0)] * len(Xs), "bf16x3", teams=teams,
                                  graph=True, groups=groups)
         for dst, X in zip(matcher.X, Xs):
@@ -682,15 +691,17 @@ def main():
     traffic = PEEL_TRAFFIC_BYTES if (C, K, NT_BATCH) == (384, 600, 60000) else None
     if batched_stage is not None and head == "bf16x3_batched":
         # one peel_multi_kernel launch covers all batches of the step; its
-        # traffic is the per-batch ncu figure times the batches (same sizes)
+        # traffic is the ncu figure of that launch (20 batches), scaled by the
+        # batches when the step has another count (same sizes)
         t_b = batched_stage["peel"] * 1e-3
+        traffic_m = PEEL_MULTI_TRAFFIC_BYTES_PER_BATCH * nb if traffic else None
         roof = {"kernel": "peel_multi_kernel", "bound": "hbm",
                 "achieved": bytes_peel / t_b / 1e9, "peak": hbm, "unit": "GB/s",
                 "frac": bytes_peel / t_b / 1e9 / hbm,
-                "traffic": traffic * nb if traffic else None, "peak_source": peak_kind,
+                "traffic": traffic_m, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": bytes_peel,
                 "no_reuse_bytes_per_launch": bytes_noreuse,
-                "traffic_gbs": (traffic * nb / t_b / 1e9 if traffic else None),
+                "traffic_gbs": (traffic_m / t_b / 1e9 if traffic_m else None),
                 "ms_per_launch": batched_stage["peel"], "batches_per_launch": nb}
     elif stage["peel"] >= stage["project"]:
         roof = {"kernel": "peel_kernel", "bound": "hbm", "achieved": peel_gbs, "peak": hbm,

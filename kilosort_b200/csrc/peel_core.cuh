@@ -34,8 +34,8 @@
 //   UPDATE  every block computes the exclusive prefix of the chunk counts (a
 //           peak's global index in the iteration) and of the dirty bitmap.
 //           Records are written in (iteration, tau) order.  Warps take work
-//           items (dirty block in column order, row range) round-robin, the
-//           last round from a counter:
+//           items (dirty block in column order, row range) from a counter
+//           (large teams: round-robin, the last round from the counter):
 //           B[j,c] -= amp*ctc[j,k,c-tau+nt] for the peaks touching column c,
 //           even-indexed peaks first, then odd-indexed -- the order of the
 //           reference's two interleaved groups (:235-238) -- product and
@@ -59,7 +59,10 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kChunk = 256;          // detection chunk, one column per thread
 constexpr int kCol = 32;             // update block, one column per lane
 constexpr int kRowsPerWarp = 16;     // template rows in flight per lane (2 blocks per SM)
-constexpr int kItemRows = 64;        // template rows per update item (at most)
+constexpr int kItemRows = 64;        // template rows per update item, large teams (at most)
+constexpr int kItemRowsSmall = 640;  // the same, small teams: a whole block's rows per
+                                     // item (one fold per column instead of ten)
+constexpr int kStaticWarps = 1024;   // teams of at least this many warps deal items statically
 constexpr int kTouch = 8;            // peaks touching one block (more: ties)
 constexpr int kMaxChunks = 16384;
 constexpr int kMaxIters = 4096;      // iterations whose record offsets are kept
@@ -643,10 +646,11 @@ __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsi
     // there are about four per warp
     // rows per item: the split whose most loaded warp has the least work
     // (row groups of 16 plus one group's worth of per-item set-up)
+    const int item_cap = nwarps >= kStaticWarps ? kItemRows : kItemRowsSmall;
     int rows = kItemRows;
     if (ndirty > 0) {
       long long best_cost = -1;
-      for (int r = kRows; r <= kItemRows; r += kRows) {
+      for (int r = kRows; r <= item_cap; r += kRows) {
         const long long items = (long long)ndirty * ((a.K + r - 1) / r);
         const long long per_warp = (items + nwarps - 1) / nwarps;
         const long long cost = per_warp * (r / kRows + 1);
@@ -662,12 +666,16 @@ __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsi
     if (rank == 0 && tid == 0) a.itoff[it] = (int)n_out;
     unsigned long long* pcur = a.pack + (size_t)p * a.L;
     KS_TRACE(it, 3, ks_globaltimer());
-    // Items of equal cost.  All but the last round are dealt round-robin
-    // (consecutive items -- neighbouring blocks, which share the slabs of their
-    // peaks -- run concurrently); the rest go to whichever warp asks first, so
-    // warps that ran into slower memory take fewer of them.
+    // Items go to warps in item order, so consecutive items (neighbouring
+    // blocks, which share the slabs of their peaks) run at about the same
+    // time.  A small team takes every item from the counter: warps that ran
+    // into slower memory take fewer of them (a static deal left the blocks
+    // of a 14-block team up to 20 % of an iteration apart at the closing
+    // barrier).  A large team deals all but its last round round-robin, so
+    // thousands of warps do not queue on one counter.
     const long long rounds = n_items / nwarps;
-    const long long n_static = rounds > 1 ? (rounds - 1) * nwarps : 0;
+    const long long n_static =
+        (nwarps >= kStaticWarps && rounds > 1) ? (rounds - 1) * nwarps : 0;
     for (long long w = gwarp; w < n_static; w += nwarps) {
       const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
       const int r = (int)(w % rgroups);
