@@ -154,11 +154,12 @@ __device__ __forceinline__ void peel_multi_body(const MultiParams& p, char* smem
       rs.xl_tau = xl;
       rs.xl_k = xl + kWarps * kXList;
       rs.xl_amp = reinterpret_cast<float*>(xl + 2 * kWarps * kXList);
+      rs.xt = nullptr;
       const int xg = (sa.C + 31) / 32;
       const long long n_items = (long long)sa.nblk * xg;
       for (long long w = (long long)rank * kWarps + warp; w < n_items;
            w += (long long)p.team_size * kWarps)
-        residual_item(sa, rs, o.iters, o.n_out, (int)(w / xg), (int)(w % xg), lane, warp);
+        residual_item<false>(sa, rs, o.iters, o.n_out, (int)(w / xg), (int)(w % xg), lane, warp);
     }
   }
 }

@@ -718,11 +718,14 @@ __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
   run_peel<kRowsPerWarp>(a, s, blockIdx.x, gridDim.x, epoch);
 }
 
+constexpr int kXTile = kCol * (kCol + 1);   // floats of one warp's transpose tile
+
 struct ResSmem {
   const float* W;  // Wt[t][8]: the basis transposed, components padded to 8
   int* xl_tau;     // warps*kXList
   int* xl_k;
   float* xl_amp;
+  float* xt;       // warps*kXTile (tiled form only): 32 channels x 33 floats per warp
 };
 
 // ---------------------------------------------------------------- RESIDUAL
@@ -806,7 +809,12 @@ __device__ int load_residual_list(const PeelArgs& a, const ResSmem& s, int blk, 
 
 // Residual of block blk for channels [32*cg, 32*cg + 32): lanes run over
 // channels, each lane keeps its 32 residual values in registers while the
-// listed spikes are subtracted in record order.
+// listed spikes are subtracted in record order.  kTiled: the 32 x 32 tile
+// moves a channel row at a time (lanes over columns, one coalesced access
+// each) through a transpose in shared memory, instead of each lane touching
+// its own row 32 times; the batched peel, whose update phase gains more from
+// the L1 that this shared memory would take, uses the direct form.
+template <bool kTiled>
 __device__ void residual_item(const PeelArgs& a, const ResSmem& s, int n_iter, long long n_out,
                               int blk, int cg, int lane, int warp) {
   const int c0 = blk * kCol;
@@ -819,9 +827,26 @@ __device__ void residual_item(const PeelArgs& a, const ResSmem& s, int n_iter, l
   if (total == 0) return;
   const int ncol = min(kCol, a.L - c0);
   float* xrow = a.Xres + (long long)c * a.L + c0;
+  float* xt = kTiled ? s.xt + warp * kXTile : nullptr;
+  const int cbase = cg * 32;
+  const bool colok = lane < ncol;
   float x[kCol];
+  if (kTiled) {
+    {
+      float v[kCol];
 #pragma unroll
-  for (int j = 0; j < kCol; ++j) x[j] = (chok && j < ncol) ? xrow[j] : 0.f;
+      for (int r = 0; r < kCol; ++r)
+        v[r] = (colok && cbase + r < a.C) ? a.Xres[(long long)(cbase + r) * a.L + c0 + lane] : 0.f;
+#pragma unroll
+      for (int r = 0; r < kCol; ++r) xt[r * (kCol + 1) + lane] = v[r];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kCol; ++j) x[j] = xt[lane * (kCol + 1) + j];
+  } else {
+#pragma unroll
+    for (int j = 0; j < kCol; ++j) x[j] = (chok && j < ncol) ? xrow[j] : 0.f;
+  }
   const int epochs = (total + kXList - 1) / kXList;
   for (int ep = 0; ep < epochs; ++ep) {
     if (ep > 0) gather_residual(a, s, n_iter, n_out, c0, ep * kXList, lane, warp);
@@ -852,9 +877,20 @@ __device__ void residual_item(const PeelArgs& a, const ResSmem& s, int n_iter, l
       }
     }
   }
+  if (kTiled) {
+    __syncwarp();
 #pragma unroll
-  for (int j = 0; j < kCol; ++j)
-    if (chok && j < ncol) xrow[j] = x[j];
+    for (int j = 0; j < kCol; ++j) xt[lane * (kCol + 1) + j] = x[j];
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < kCol; ++r)
+      if (colok && cbase + r < a.C)
+        a.Xres[(long long)(cbase + r) * a.L + c0 + lane] = xt[r * (kCol + 1) + lane];
+  } else {
+#pragma unroll
+    for (int j = 0; j < kCol; ++j)
+      if (chok && j < ncol) xrow[j] = x[j];
+  }
 }
 
 constexpr int kResThreads = 256;
@@ -871,6 +907,7 @@ ks_residual_kernel(PeelArgs a) {
   s.xl_tau = reinterpret_cast<int*>(sW + 8 * a.nt);
   s.xl_k = s.xl_tau + kResWarps * kXList;
   s.xl_amp = reinterpret_cast<float*>(s.xl_k + kResWarps * kXList);
+  s.xt = s.xl_amp + kResWarps * kXList;
   stage_basis_t8(a.W, a.P, a.nt, sW, kResThreads);
   __syncthreads();
   const long long n_out = a.info[0];
@@ -882,13 +919,14 @@ ks_residual_kernel(PeelArgs a) {
   const long long n_items = (long long)a.nblk * xg;
   const long long w = (long long)blockIdx.x * kResWarps + warp;
   if (w >= n_items) return;
-  residual_item(a, s, n_iter, n_out, (int)(w / xg), (int)(w % xg), lane, warp);
+  residual_item<true>(a, s, n_iter, n_out, (int)(w / xg), (int)(w % xg), lane, warp);
 }
 
 size_t residual_smem_bytes(int P, int nt) {
   (void)P;
   return sizeof(float) * 8 * (size_t)nt +
-         (size_t)kResWarps * kXList * (2 * sizeof(int) + sizeof(float));
+         (size_t)kResWarps * kXList * (2 * sizeof(int) + sizeof(float)) +
+         sizeof(float) * (size_t)kResWarps * kXTile;
 }
 
 __global__ void ks_nm_pair_kernel(const float* __restrict__ nm, int K, float2* __restrict__ nmi) {
