@@ -116,7 +116,8 @@ def extract_sharded(ops, bfile, U, device=None, dst: int = 0, group=None,
         features = features or f
     start, stop = batch_range(int(bfile.n_batches), world, rank)
     st, tF = tm.extract_batches(ops, bfile, np.arange(start, stop, dtype=np.int64), U, ctc,
-                                match, features, progress_bar)
+                                match, features, progress_bar,
+                                read_ahead=bool(ops.get("read_ahead", True)))
     if distributed:
         st, tF = _gather_rows(st, tF, dst, group)
         if rank != dst:

@@ -15,7 +15,10 @@ path: inputs must be float32 CUDA tensors on a B200.
 Extra ``ops`` keys understood here (the reference ignores them):
 ``projection`` -- ``"fp32"`` (plain FP32 contraction, the default) or
 ``"bf16x3"`` (split-BF16 on tensor cores); ``spike_capacity`` -- spike rows
-per batch (default 100000, the reference's fixed buffer size).
+per batch (default 100000, the reference's fixed buffer size);
+``read_ahead`` -- `extract` reads the next batch while matching the current
+one (default True; set False for a batch source whose
+``padded_batch_to_torch`` returns the same buffer on every call).
 """
 from __future__ import annotations
 
@@ -419,7 +422,10 @@ def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=N
     ``match(X, U, ctc, device)`` returns ``(st, amps, th_amps, Xres)`` and
     ``features(Xres, st, amps)`` the ``[N, nC, P]`` features of one batch.
     With ``read_ahead`` the next batch is read while the current one is
-    matched (the same batches in the same order).  Rows are gathered per
+    matched (the same batches in the same order), so the batch source must
+    return a new tensor per call (the reference's ``BinaryFiltered`` does); a
+    source that refills one buffer needs ``read_ahead=False``
+    (``ops['read_ahead'] = False`` through `extract`).  Rows are gathered per
     batch and joined once at the end (the reference grows preallocated
     buffers of 10**6 rows; the returned rows are the same).
     """
@@ -496,7 +502,8 @@ def extract(ops, bfile, U, device=torch.device("cuda"), progress_bar=None):
     iCCd = iCC.to(U.device).contiguous()
     match, features = _match_features(ops, W, iCCd, iU, Ucc)
     batches = np.arange(bfile.n_batches, dtype=np.int64)
-    st, tF = extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar)
+    st, tF = extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar,
+                             read_ahead=bool(ops.get("read_ahead", True)))
     st, tF = sort_spikes(st, tF)
     return st, tF, ops
 

@@ -215,3 +215,24 @@ def test_extract_read_ahead_equals_reference_extract():
         st, tF = tm.sort_spikes(st, tF)
         np.testing.assert_array_equal(st, g["st"])
         np.testing.assert_array_equal(tF.numpy(), g["tF"])
+
+
+class _RefillingSource(synth.SyntheticBinary):
+    """A batch source that refills one buffer on every call."""
+
+    def padded_batch_to_torch(self, ibatch, ops=None):
+        x = torch.from_numpy(np.ascontiguousarray(self.rec.batch(int(ibatch))))
+        if not hasattr(self, "_buf"):
+            self._buf = torch.empty_like(x)
+        return self._buf.copy_(x)
+
+
+def test_refilling_source_without_read_ahead_equals_reference_extract():
+    g, rec = _golden_case()
+    ops = dict(_ops(rec), read_ahead=False)
+    prepare, match, features = _oracle_fns(rec, ops)
+    st, tF, _ = sharding.extract_sharded(ops, _RefillingSource(rec, device="cpu"),
+                                         torch.from_numpy(rec.U), device="cpu",
+                                         prepare=prepare, match=match, features=features)
+    np.testing.assert_array_equal(st, g["st"])
+    np.testing.assert_array_equal(tF.numpy(), g["tF"])
