@@ -98,7 +98,11 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        # raw samples go to KS_CLOCKS_DIR (default: the system temp directory);
+        # the JSON line carries their summary
+        import tempfile
+        self.path = os.path.join(os.environ.get("KS_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"clocks_bench_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
