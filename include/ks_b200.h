@@ -161,19 +161,22 @@ KS_API int ks_ctc(const float* U, const float* W, int64_t K, int64_t P, int64_t 
  * a batch, for instance an acquisition loop that must not call cudaMalloc on
  * its hot path (it can synchronise the device and has no latency bound), or a
  * host plugin that is handed device buffers but owns no device allocator.
- * Same computation and outputs as ks_peel with a tiled score matrix
- * (KS_B_TILED) and transposed cross-correlations (KS_CTC_KJL); instead of a
- * workspace it uses a fixed 7 MiB array in the library's device image (one
- * per GPU that loads the library, held until the process exits), so batches
- * are limited to KS_PEEL_STATIC_MAX_L padded samples (longer ones return
- * KS_ERR_UNSUPPORTED).  The first call on a device looks the array's device
- * address up; make that call before any stream capture.  Every call shares
- * the array (it keeps the last call's contents; what must start at zero is
- * cleared per call), so calls whose kernels overlap on the GPU race and must
- * be serialised by the caller.  No counterpart in the reference: it adds a
- * way to run kilosort/template_matching.py:183-244 without allocation.
+ * Same outputs as ks_peel with a tiled score matrix (KS_B_TILED) and
+ * transposed cross-correlations (KS_CTC_KJL); instead of a workspace it uses
+ * a fixed 7 MiB array in the library's device image (one per GPU that loads
+ * the library, held until the process exits).  The array holds batches of up
+ * to KS_PEEL_STATIC_MAX_L padded samples with up to KS_PEEL_STATIC_MAX_K
+ * templates (shorter batches leave room for more); a shape whose scratch does
+ * not fit returns KS_ERR_UNSUPPORTED with a message naming both limits.  A
+ * call on a stream that is not capturing looks the array's device address up
+ * (and caches it); inside a stream capture the cached address is used, so make
+ * the first call on a device before any capture.  Every call shares the array
+ * (it keeps the last call's contents; what must start at zero is cleared per
+ * call), so calls whose kernels overlap on the GPU race and must be
+ * serialised by the caller.  No counterpart in the reference.
  */
 #define KS_PEEL_STATIC_MAX_L 131072
+#define KS_PEEL_STATIC_MAX_K 56896
 KS_API int ks_peel_static(float* Bt, float* Xres, const float* U, const float* W,
                           const float* ctcT, const float* nm, int64_t C, int64_t L,
                           int64_t K, int64_t P, int64_t nt, float th2,

@@ -38,6 +38,9 @@ struct MultiRec {
   const float* ctcT;
   const float* nm;
   const float2* nmi;
+  const int* rperm;             // group order of the grouped update
+  const float* mg;              // its product bounds [K][ng]
+  const float2* nmip;           // {nm, 1/nm} in group order
   int C, K, P, nt;
   float th2;
   int max_peels;
@@ -66,7 +69,7 @@ struct MultiParams {
   size_t team_bytes;
   unsigned long long limit_ns;
   const int* upstream_err;
-  size_t peel_smem;             // dynamic shared bytes of the peel (lists follow)
+  size_t peel_smem;             // dynamic shared bytes of the peel
 };
 
 __device__ void fill_args(const MultiParams& p, int b, char* team, PeelArgs& a) {
@@ -92,7 +95,10 @@ __device__ void fill_args(const MultiParams& p, int b, char* team, PeelArgs& a) 
   a.amps = mb.amps;
   a.th_amps = mb.th_amps;
   a.info = mb.info;
-  bind_scratch(a, team, mb.lists);
+  bind_scratch(a, team, mb.lists, true);
+  a.rperm = r.rperm;
+  a.mg = r.mg;
+  a.nmip = r.nmip;
   a.limit_ns = p.limit_ns;
   a.upstream_err = p.upstream_err;
 #ifdef KS_PEEL_TRACE
@@ -135,31 +141,32 @@ __device__ __forceinline__ void peel_multi_body(const MultiParams& p, char* smem
   const int n_teams = gridDim.x / p.team_size;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   char* tbase = p.teams + (size_t)team * p.team_bytes;
-  // per-warp residual lists after the peel's own shared memory
-  int* xl = reinterpret_cast<int*>(smem_raw + p.peel_smem);
   unsigned epoch = 0;
   for (int i = team; i < p.n_batches; i += n_teams) {
     __syncthreads();
     if (threadIdx.x == 0) fill_args(p, p.order[i], tbase, sa);
     __syncthreads();
-    const Smem s = carve_smem(sa, smem_raw);
-    const PeelOutcome o = run_peel<kRows>(sa, s, rank, (unsigned)p.team_size, epoch);
+    const Smem s = carve_smem(sa, smem_raw, true);
+    const PeelOutcome o = run_peel<kRows, true>(sa, s, rank, (unsigned)p.team_size, epoch);
     if (o.status != KS_OK) {
       if (o.status == KS_ERR_OVERFLOW) continue;   // that batch only
       break;
     }
     if (o.n_out > 0) {
+      // the residual's per-warp lists and transpose tiles use the update's
+      // stage tiles, which the peel of this batch no longer needs
+      int* xl = reinterpret_cast<int*>(s.stage);
       ResSmem rs;
       rs.W = s.W;
       rs.xl_tau = xl;
       rs.xl_k = xl + kWarps * kXList;
       rs.xl_amp = reinterpret_cast<float*>(xl + 2 * kWarps * kXList);
-      rs.xt = nullptr;
+      rs.xt = reinterpret_cast<float*>(xl + 3 * kWarps * kXList);
       const int xg = (sa.C + 31) / 32;
       const long long n_items = (long long)sa.nblk * xg;
       for (long long w = (long long)rank * kWarps + warp; w < n_items;
            w += (long long)p.team_size * kWarps)
-        residual_item<false>(sa, rs, o.iters, o.n_out, (int)(w / xg), (int)(w % xg), lane, warp);
+        residual_item<true>(sa, rs, o.iters, o.n_out, (int)(w / xg), (int)(w % xg), lane, warp);
     }
   }
 }
@@ -167,7 +174,7 @@ __device__ __forceinline__ void peel_multi_body(const MultiParams& p, char* smem
 // -------------------------------------------------------------- host layout
 struct RecPlan {
   int64_t Q, Kpad, rows;          // rows: stacked Lpad of its batches (split form)
-  size_t nm, nmi, uhi, ulo, uf, yhi, ylo;
+  size_t nm, nmi, groups, uhi, ulo, uf, yhi, ylo;
 };
 
 struct BatchPlan {
@@ -179,7 +186,7 @@ struct Plan {
   std::vector<RecPlan> rec;
   std::vector<BatchPlan> bat;
   size_t ctl, yf, teams, team_bytes, bytes;
-  int64_t maxL, maxYf;
+  int64_t maxL, maxK, maxYf;
   int n_teams;
 };
 
@@ -195,6 +202,7 @@ int make_plan(const ks_rec_desc* recs, int64_t n_recs, const ks_batch_desc* batc
   pl.rec.assign(n_recs, RecPlan{});
   pl.bat.assign(n_batches, BatchPlan{});
   pl.maxL = 0;
+  pl.maxK = 0;
   pl.maxYf = 0;
   for (int64_t r = 0; r < n_recs; ++r) {
     const ks_rec_desc& d = recs[r];
@@ -220,6 +228,7 @@ int make_plan(const ks_rec_desc* recs, int64_t n_recs, const ks_batch_desc* batc
     if (pl.rec[d.rec].rows > 0x7fffffffLL)
       return fail(KS_ERR_UNSUPPORTED, "ks_match_batches: too many samples for one recording");
     pl.maxL = std::max(pl.maxL, d.L);
+    pl.maxK = std::max(pl.maxK, r.K);
     pl.maxYf = std::max(pl.maxYf, pl.bat[b].Lpad * pl.rec[d.rec].Q);
   }
   size_t o = 0;
@@ -234,6 +243,7 @@ int make_plan(const ks_rec_desc* recs, int64_t n_recs, const ks_batch_desc* batc
     const ks_rec_desc& d = recs[r];
     rp.nm = take(sizeof(float) * d.K);
     rp.nmi = take(sizeof(float2) * d.K);
+    rp.groups = take(group_tables_bytes(d.K));
     if (precision == KS_PROJ_BF16X3) {
       rp.uhi = take(2 * (size_t)rp.Kpad * rp.Q);
       rp.ulo = take(2 * (size_t)rp.Kpad * rp.Q);
@@ -253,7 +263,7 @@ int make_plan(const ks_rec_desc* recs, int64_t n_recs, const ks_batch_desc* batc
   if (t <= 0) t = std::min<int64_t>(8, std::max<int64_t>(1, n_batches / 4));
   t = std::min<int64_t>(t, n_batches);
   pl.n_teams = (int)t;
-  pl.team_bytes = al256(team_layout(pl.maxL).bytes);
+  pl.team_bytes = al256(team_layout(pl.maxL, pl.maxK).bytes);
   pl.teams = take(pl.team_bytes * (size_t)t);
   pl.bytes = o;
   return KS_OK;
@@ -334,6 +344,9 @@ extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
     float* nm = reinterpret_cast<float*>(base + rp.nm);
     if ((rc = launch_template_energy(d.U, d.K, d.P, d.C, nm, s))) return rc;
     if ((rc = launch_nm_pairs(nm, d.K, reinterpret_cast<float2*>(base + rp.nmi), s))) return rc;
+    if ((rc = launch_group_setup(d.U, d.ctcT, reinterpret_cast<const float2*>(base + rp.nmi), d.K,
+                                 d.P, d.C, d.nt, base + rp.groups, s)))
+      return rc;
     if (precision == KS_PROJ_BF16X3)
       rc = launch_reorder_templates(d.U, d.K, d.P, d.C, rp.Kpad, rp.Q, nullptr,
                                     reinterpret_cast<__nv_bfloat16*>(base + rp.uhi),
@@ -368,6 +381,7 @@ extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
     m.ctcT = d.ctcT;
     m.nm = reinterpret_cast<const float*>(base + pl.rec[r].nm);
     m.nmi = reinterpret_cast<const float2*>(base + pl.rec[r].nmi);
+    group_tables(base + pl.rec[r].groups, d.K, &m.rperm, &m.mg, &m.nmip);
     m.C = (int)d.C;
     m.K = (int)d.K;
     m.P = (int)d.P;
@@ -393,7 +407,7 @@ extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
     const int nchunks = (int)((d.L + kChunk - 1) / kChunk);
     const int nblk = (int)((d.L + kCol - 1) / kCol);
     const int nwords = (nblk + 31) / 32;
-    smem = std::max(smem, smem_bytes((int)r.P, (int)r.nt, nchunks, nwords));
+    smem = std::max(smem, smem_bytes((int)r.P, (int)r.nt, nchunks, nwords, true));
   }
   mp.teams = base + pl.teams;
   mp.team_bytes = pl.team_bytes;
@@ -401,7 +415,6 @@ extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
   mp.upstream_err = precision == KS_PROJ_BF16X3 ? gemm_err : nullptr;
   smem = (smem + 15) & ~size_t(15);
   mp.peel_smem = smem;
-  smem += (size_t)kWarps * kXList * (2 * sizeof(int) + sizeof(float));   // residual lists
   const PeelVariant pv = peel_variant(pipelined);
   cudaFuncAttributes fa;
   KS_CUDA(cudaFuncGetAttributes(&fa, pv.kernel));

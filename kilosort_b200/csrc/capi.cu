@@ -99,7 +99,7 @@ static MatchLayout match_layout(int64_t C, int64_t L, int64_t K, int64_t P, int6
   m.ctc_off = off;
   off += ctcT_bytes(K, nt, ctc_layout);
   m.peel_off = off;
-  off = align256(off + peel_scratch_size(L, K));
+  off = align256(off + peel_scratch_size(L, K, true));
   m.bytes = off;
   return m;
 }
@@ -118,7 +118,7 @@ static PeelWsLayout peel_ws_layout(int64_t L, int64_t K, int64_t nt, int b_layou
   m.ctc_off = off;
   off += ctcT_bytes(K, nt, ctc_layout);
   m.peel_off = off;
-  off = align256(off + peel_scratch_size(L, K));
+  off = align256(off + peel_scratch_size(L, K, true));
   m.bytes = off;
   return m;
 }
@@ -222,7 +222,7 @@ int ks_peel(float* B, int64_t ldb, int b_layout, float* Xres, const float* U, co
   }
   rc = launch_peel_tiled(Bt, Xres, U, W, ctcT, nm, C, L, K, P, nt, th2, max_peels, capacity,
                          st, amps, th_amps, info, base + m.peel_off, m.bytes - m.peel_off, s,
-                         wait_limit_ns(), nullptr);
+                         wait_limit_ns(), nullptr, true);
   if (rc) return rc;
   return b_layout == KS_B_ROWS ? launch_untile_rows(Bt, K, L, B, ldb, s) : KS_OK;
 }
@@ -273,7 +273,7 @@ int ks_run_matching(const float* X, const float* U, const float* W, const float*
   return launch_peel_tiled(Bt, Xres, U, W, ctcT, nm, C, L, K, P, nt, th2, max_peels,
                            capacity, st, amps, th_amps, info, base + m.peel_off,
                            m.bytes - m.peel_off, s, wait_limit_ns(),
-                           reinterpret_cast<const int*>(base + m.proj_off));
+                           reinterpret_cast<const int*>(base + m.proj_off), true);
 }
 
 int ks_ctc_transpose(const float* ctc, int64_t K, int64_t nt, float* ctcT, void* stream) {

@@ -4,8 +4,67 @@
 
 namespace ks {
 
-size_t peel_scratch_size(int64_t L, int64_t K) {
-  return al256(team_layout(L).bytes) + al256(list_layout(L).bytes) + al256(8 * (size_t)K);
+// Scratch of one single-batch peel: [team region] [lists] [nmi 8K], and for
+// the grouped update its tables (group_tables_bytes).
+// Tables of the grouped update: [rperm 4K] [key 4K] [mg 4*K*ng] [nmip 8K].
+static size_t group_setup_bytes(int64_t K) {
+  return al256(4 * (size_t)K) + al256(4 * (size_t)K) + al256(4 * (size_t)K * n_groups(K)) +
+         al256(8 * (size_t)K);
+}
+
+size_t peel_scratch_size(int64_t L, int64_t K, bool grouped) {
+  return al256(team_layout(L, grouped ? K : 0).bytes) + al256(list_layout(L).bytes) +
+         al256(8 * (size_t)K) + (grouped ? group_setup_bytes(K) : 0);
+}
+
+size_t group_tables_bytes(int64_t K) { return group_setup_bytes(K); }
+
+struct GroupTables {
+  int* rperm;
+  float* key;
+  float* mg;
+  float2* nmip;
+};
+
+static GroupTables group_tables_at(void* tables, int64_t K) {
+  char* base = static_cast<char*>(tables);
+  const size_t k4 = al256(4 * (size_t)K);
+  GroupTables t;
+  t.rperm = reinterpret_cast<int*>(base);
+  t.key = reinterpret_cast<float*>(base + k4);
+  t.mg = reinterpret_cast<float*>(base + 2 * k4);
+  t.nmip = reinterpret_cast<float2*>(base + 2 * k4 + al256(4 * (size_t)K * n_groups(K)));
+  return t;
+}
+
+// Group order, product bounds and permuted {nm, 1/nm} of the grouped update
+// for one template set (ctcT in the transposed layout, nmi from
+// launch_nm_pairs), written into tables (group_tables_bytes(K)).
+int launch_group_setup(const float* U, const float* ctcT, const float2* nmi, int64_t K,
+                       int64_t P, int64_t C, int64_t nt, void* tables, cudaStream_t stream) {
+  const GroupTables t = group_tables_at(tables, K);
+  const int ng = n_groups(K);
+  ks_template_key_kernel<<<(unsigned)((K * 32 + 255) / 256), 256, 0, stream>>>(U, (int)K, (int)P,
+                                                                              (int)C, t.key);
+  KS_CUDA(cudaGetLastError());
+  ks_group_order_kernel<<<(unsigned)((K + 255) / 256), 256, 0, stream>>>(t.key, (int)K, t.rperm);
+  KS_CUDA(cudaGetLastError());
+  const long long items = K * (long long)ng;
+  ks_group_bound_kernel<<<(unsigned)std::min<long long>(items, 1 << 20), 256, 0, stream>>>(
+      ctcT, t.rperm, (int)K, (int)(2 * nt + 1), ng, t.mg);
+  KS_CUDA(cudaGetLastError());
+  ks_group_nmi_kernel<<<(unsigned)((K + 255) / 256), 256, 0, stream>>>(nmi, t.rperm, (int)K,
+                                                                      t.nmip);
+  KS_CUDA(cudaGetLastError());
+  return KS_OK;
+}
+
+void group_tables(void* tables, int64_t K, const int** rperm, const float** mg,
+                  const float2** nmip) {
+  const GroupTables t = group_tables_at(tables, K);
+  *rperm = t.rperm;
+  *mg = t.mg;
+  *nmip = t.nmip;
 }
 
 int64_t tiled_rows_floats(int64_t L, int64_t K) { return ((L + kCol - 1) / kCol) * K * kCol; }
@@ -78,12 +137,12 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
                       int64_t P, int64_t nt, float th2, int64_t max_peels,
                       int64_t capacity, int64_t* st, float* amps, float* th_amps,
                       int64_t* info, void* ws, size_t ws_bytes, cudaStream_t stream,
-                      unsigned long long limit_ns, const int* upstream_err) {
+                      unsigned long long limit_ns, const int* upstream_err, bool grouped) {
   if (!Bt || !Xres || !U || !W || !ctcT || !nm || !st || !amps || !th_amps || !info)
     return fail(KS_ERR_ARG, "ks_peel: null pointer");
   int rc = check_peel_shape(C, L, K, P, nt, th2, max_peels, capacity);
   if (rc) return rc;
-  if (ws_bytes < peel_scratch_size(L, K) || !ws)
+  if (ws_bytes < peel_scratch_size(L, K, grouped) || !ws)
     return fail(KS_ERR_WORKSPACE, "ks_peel: workspace too small");
 
   DeviceInfo dev;
@@ -99,26 +158,33 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
   a.st = reinterpret_cast<long long*>(st); a.amps = amps; a.th_amps = th_amps;
   a.info = reinterpret_cast<long long*>(info);
   char* base = static_cast<char*>(ws);
-  const size_t team_bytes = al256(team_layout(L).bytes);
+  const size_t team_bytes = al256(team_layout(L, grouped ? K : 0).bytes);
   const size_t list_bytes = al256(list_layout(L).bytes);
-  bind_scratch(a, base, base + team_bytes);
+  bind_scratch(a, base, base + team_bytes, grouped);
   float2* nmi = reinterpret_cast<float2*>(base + team_bytes + list_bytes);
   a.nmi = nmi;
+  void* tables = base + team_bytes + list_bytes + al256(8 * (size_t)K);
+  if (grouped) group_tables(tables, K, &a.rperm, &a.mg, &a.nmip);
   a.limit_ns = limit_ns;
   a.upstream_err = upstream_err;
 #ifdef KS_PEEL_TRACE
   a.trace = 1;
 #endif
 
-  const size_t smem = smem_bytes(a.P, a.nt, a.nchunks, a.nwords);
+  const size_t smem = smem_bytes(a.P, a.nt, a.nchunks, a.nwords, grouped);
   if (smem > dev.smem_optin) return fail(KS_ERR_UNSUPPORTED, "ks_peel: batch too long for shared memory");
+  void (*kernel)(PeelArgs) = grouped ? peel_kernel<true> : peel_kernel<false>;
   int occ = 0;
-  rc = peel_occupancy(dev, smem, (const void*)peel_kernel, &occ);
+  rc = peel_occupancy(dev, smem, (const void*)kernel, &occ);
   if (rc) return rc;
   const int grid = dev.sm_count * occ;
   KS_CUDA(cudaMemsetAsync(base, 0, 256, stream));       // barrier count and error word
   rc = launch_nm_pairs(nm, K, nmi, stream);
   if (rc) return rc;
+  if (grouped) {
+    rc = launch_group_setup(U, ctcT, nmi, K, P, C, nt, tables, stream);
+    if (rc) return rc;
+  }
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -130,7 +196,7 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   trace_mark(2, stream);
-  KS_CUDA(cudaLaunchKernelEx(&cfg, peel_kernel, a));
+  KS_CUDA(cudaLaunchKernelEx(&cfg, kernel, a));
   trace_mark(3, stream);
   // residual updates of all recorded spikes
   const long long n_res = (long long)a.nblk * ((C + 31) / 32);

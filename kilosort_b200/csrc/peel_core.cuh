@@ -54,11 +54,11 @@
 
 namespace {
 
-constexpr int kThreads = 512;
+constexpr int kThreads = 384;
 constexpr int kWarps = kThreads / 32;
 constexpr int kChunk = 256;          // detection chunk, one column per thread
 constexpr int kCol = 32;             // update block, one column per lane
-constexpr int kRowsPerWarp = 16;     // template rows in flight per lane (2 blocks per SM)
+constexpr int kRowsPerWarp = 16;     // template rows in flight per lane (ungrouped update)
 constexpr int kItemRows = 64;        // template rows per update item, large teams (at most)
 constexpr int kItemRowsSmall = 640;  // the same, small teams: a whole block's rows per
                                      // item (one fold per column instead of ten)
@@ -69,6 +69,8 @@ constexpr int kMaxIters = 4096;      // iterations whose record offsets are kept
 constexpr int kMaxTemplates = 65536; // templates of one batch
 constexpr int kXList = 64;           // residual list entries per warp and epoch
 constexpr int kXCap = 32;            // spikes recorded per block for the residual
+constexpr int kGroup = 32;           // template rows of one group (grouped update)
+constexpr int kInitGroups = 2;       // groups per item of the initial scoring
 
 // Phase timeline for profiling builds (-DKS_PEEL_TRACE): block 0 writes
 // %globaltimer stamps to info[8 + 8*it + slot]; the caller sizes info.
@@ -128,13 +130,28 @@ struct PeelArgs {
   int* tcount;                // [2][nblk]
   Touch* touch;               // [2][nblk * kTouch]
   unsigned* dbits;            // [2][nwords]
-  unsigned* wctr;             // [2] work counters
+  unsigned* wctr;             // [6] work counters by iteration parity: [0,1] update
+                              //     items, [2,3] grouped units written, [4,5] taken
   int* itoff;                 // [kMaxIters] first record of each iteration
   int* xcount;                // [nblk] spikes whose residual window meets the block
   int* xlist;                 // [nblk * kXCap] their record indices (unordered)
   unsigned* bar;              // barrier arrival count (monotonic)
   int* err;
   const int* upstream_err;    // error word of the producer of Bt (may be null)
+  // grouped update (null rperm: every row of a touched column is rewritten)
+  const int* rperm;           // [K] template rows in group order (group g: rows
+                              //     rperm[32g .. 32g+31])
+  const float2* nmip;         // [K] {nm, 1/nm} in group order, nmip[r] = nmi[rperm[r]]
+  const float* mg;            // [K][ng] largest |ctcT[k][j][l]| over the rows j
+                              //     of group g and all lags
+  unsigned long long* gbest;  // [nblk][ng][32] packed best score of each group
+                              //     per column (pack_score)
+  unsigned char* gexp;        // [nblk][ng][32] smallest exponent field of |B|
+                              //     over each group's rows per column (noop_expo)
+  int* blist;                 // [nblk][32] a dirty block's ordered touch list for
+                              //     its units: n, tau[kTouch], k[kTouch], amp bits
+  uint2* units;               // [nblk*ng] (block << 11 | group, columns to process)
+  int ng;                     // groups, ceil(K / kGroup)
   int nchunks, nblk, nwords;
   int trace;                  // profiling builds: 1 where info has room for the timeline
   unsigned long long limit_ns;
@@ -152,6 +169,11 @@ struct Smem {
   int* tl_tau;     // kWarps*kTouch   ordered touch list of each warp's item
   int* tl_k;       // kWarps*kTouch
   float* tl_amp;   // kWarps*kTouch
+  unsigned char* eb;  // kWarps*kTouch*32  bound exponents of a warp's touching peaks
+  float* stage;       // kWarps*2*kGroup*32 (grouped update only): a warp's tile of
+                      //   B rows [kGroup][32] and of ctc rows [kGroup][32]
+  float2* rtab;       // kWarps*kGroup (grouped update only): row index bits and nm
+                      //   of the rows of the group a warp processes
 };
 
 // Wt[t][p] = W[p][t] for p < P, 0 for P <= p < 8: each tap's components are
@@ -164,7 +186,7 @@ __device__ __forceinline__ void stage_basis_t8(const float* W, int P, int nt, fl
   }
 }
 
-__device__ __forceinline__ Smem carve_smem(const PeelArgs& a, char* base) {
+__device__ __forceinline__ Smem carve_smem(const PeelArgs& a, char* base, bool grouped) {
   Smem s;
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -184,17 +206,23 @@ __device__ __forceinline__ Smem carve_smem(const PeelArgs& a, char* base) {
   s.tl_tau = reinterpret_cast<int*>(take(sizeof(int) * kWarps * kTouch));
   s.tl_k = reinterpret_cast<int*>(take(sizeof(int) * kWarps * kTouch));
   s.tl_amp = reinterpret_cast<float*>(take(sizeof(float) * kWarps * kTouch));
+  s.eb = reinterpret_cast<unsigned char*>(take(kWarps * kTouch * 32));
+  s.stage = grouped ? reinterpret_cast<float*>(take(sizeof(float) * kWarps * 2 * kGroup * 32))
+                    : nullptr;
+  s.rtab = grouped ? reinterpret_cast<float2*>(take(sizeof(float2) * kWarps * kGroup)) : nullptr;
   return s;
 }
 
-size_t smem_bytes(int P, int nt, int nchunks, int nwords) {
+size_t smem_bytes(int P, int nt, int nchunks, int nwords, bool grouped) {
   auto r = [](size_t b) { return (b + 15) & ~size_t(15); };
   const size_t wn = kChunk + 2 * (size_t)nt;
   (void)P;
   return r(sizeof(float) * 8 * nt) + r(sizeof(int) * (nchunks + 1)) +
          r(sizeof(int) * (nwords + 1)) + 3 * r(sizeof(float) * wn) +
          r(sizeof(int) * kChunk) + r(sizeof(int) * (kWarps + 1)) +
-         3 * r(sizeof(int) * kWarps * kTouch);
+         3 * r(sizeof(int) * kWarps * kTouch) + r(kWarps * kTouch * 32) +
+         (grouped ? r(sizeof(float) * kWarps * 2 * kGroup * 32) + r(sizeof(float2) * kWarps * kGroup)
+                  : 0);
 }
 
 __device__ __forceinline__ unsigned long long pack_score(float cf, int j) {
@@ -519,6 +547,394 @@ __device__ void update_warp_item(const PeelArgs& a, const TouchList& tl, int blk
   }
 }
 
+// Exponent field of |x| as the no-op test reads a score: the biased exponent
+// of a normal number; 0 for zero, subnormal, infinite and NaN values, whose
+// groups then always take the exact path.
+__device__ __forceinline__ int noop_expo(float x) {
+  const int e = (int)((__float_as_uint(x) >> 23) & 0xffu);
+  return e == 255 ? 0 : e;
+}
+
+// Exponent field of a non-negative product bound (255 for infinity or NaN,
+// which never passes the test).
+__device__ __forceinline__ int bound_expo(float b) {
+  return (int)((__float_as_uint(b) >> 23) & 0xffu);
+}
+
+// cp.async global -> shared: 4 bytes (L1-allocating) and 16 bytes (L2 only),
+// and the wait for this thread's copies.
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// ----------------------------------------------------------- grouped update
+// Grouped form of update_warp_item.  The K template rows are cut into groups
+// of kGroup rows in the order rperm (templates sorted by the channel centroid
+// of their energy, so one group holds templates of neighbouring sites).
+// Before touching a group, a column decides from per-group metadata alone
+// whether the subtractions can change any of its rows:
+//   the product that a subtraction rounds, p = fl(amp * ctc[j,k,l]), has
+//   |p| <= fl(|amp| * mg[k][g]) = bnd, because |ctc[j,k,l]| <= mg[k][g] (the
+//   group's largest magnitude over rows and lags) and rounding is monotone;
+//   if bnd's exponent field Eb satisfies Eb <= gexp - 26, where gexp is the
+//   smallest exponent field of |B[j,c]| over the group's rows, then
+//   |p| < 2^(Eb-126) <= 2^(gexp-152) <= ulp(B[j,c]) / 4 for every row j of
+//   the group, so fl(B[j,c] - p) = B[j,c] exactly (also when B[j,c] is a power
+//   of two, where the spacing below it is ulp / 2), for each of the peaks
+//   touching the column in turn.
+// Zero, subnormal, infinite and NaN scores give gexp = 0, and an infinite or
+// NaN bound gives Eb = 255, so those always take the exact path.  A (column,
+// group) pair that passes is left as it is: its rows are not read, its
+// cross-correlations are not loaded and its cached best (gbest) stands.  The
+// other pairs are updated exactly as update_warp_item does (same peaks, same
+// order, same roundings), and their gbest and gexp are rewritten.  The
+// column's best is the packed maximum over all groups (larger score, then the
+// smaller template index), which equals update_warp_item's in-order fold.
+//
+// An iteration's update runs in two phases separated by a team barrier, so
+// that the uneven work (a dirty block needs anywhere from none to all of its
+// groups) is spread evenly: group_scan_block (one warp per dirty block) reads
+// only metadata, folds the cached bests of the groups its columns leave
+// alone into the column maxima and appends each group that some column must
+// process to the iteration's unit list; unit_run (units taken from a
+// counter) processes one such group tile.
+
+// Per-lane view of an ordered touch list: the first entry touching this
+// column (-1: none) and the mask of the others.
+struct LaneEntries {
+  int e0;
+  unsigned rest;
+};
+
+__device__ __forceinline__ LaneEntries lane_entries(const TouchList& tl, int c, bool colok, int nt) {
+  LaneEntries le{-1, 0u};
+  for (int e = 0; e < tl.n; ++e) {
+    const int d = c - tl.tau[e];
+    if (colok && d >= -nt && d <= nt) {
+      if (le.e0 < 0) le.e0 = e;
+      else le.rest |= 1u << e;
+    }
+  }
+  return le;
+}
+
+// One group tile (group g of block blk): when some column of the warp has nd
+// set, the warp stages the group's 32 rows of B (whole rows, 16-byte copies)
+// and every nd column stages its first touching peak's cross-correlations,
+// into the warp's shared tiles with cp.async (one round trip, no registers
+// held in flight); the columns subtract their touching peaks in application
+// order (further peaks stage their cross-correlations into the same tile),
+// write the rows back when `store`, and rewrite the group's gbest and gexp.
+// jl / nl: row index and {nm, 1/nm} of group position `lane` (rperm, nmip).
+// Returns the group's packed best for nd columns (0 otherwise).  Called by
+// the whole warp.
+//
+// The best over the group's rows is found without a division per row: with
+// approx = fl(sq * fl(1/nm)) within a relative 2^-22 of the exact quotient
+// cf = fl(sq / nm) (sq and the quotient normal), a row whose approx is below
+// (1 - 2^-20) times the largest approx m of the group cannot reach the exact
+// quotient of the row holding m, so only the rows at or above that level
+// (and rows whose approx is NaN) have their exact quotient computed and
+// folded (larger score, then the smaller template index).  When m is below
+// 2^-100 every row takes the exact path (a zero sq with a normal nm has the
+// quotient +0 and needs no division).
+__device__ unsigned long long group_tile(const PeelArgs& a, const Smem& s, const TouchList& tl,
+                                         int blk, int g, bool nd, const LaneEntries& le,
+                                         bool store, int jl, float2 nl, int lane, int warp) {
+  const int c = blk * kCol + lane;
+  const int nt = a.nt, K = a.K, nlag = 2 * nt + 1;
+  const int nrow = min(kGroup, K - g * kGroup);
+  float* Bs = s.stage + (size_t)warp * (2 * kGroup * 32);
+  float* Cs = Bs + kGroup * 32;
+  float2* rtab = s.rtab + warp * kGroup;
+  const float* brow = a.Bt + (size_t)blk * K * kCol;
+  const float* cp0 = a.ctcT;
+  float amp0 = 0.f;
+  if (le.e0 >= 0) {
+    cp0 = a.ctcT + (size_t)tl.k[le.e0] * K * nlag + (c - tl.tau[le.e0] + nt);
+    amp0 = tl.amp[le.e0];
+  }
+  const bool any_nd = __any_sync(0xffffffffu, nd);
+  const unsigned rest_any = __reduce_or_sync(0xffffffffu, nd ? le.rest : 0u);
+  __syncwarp();                       // earlier readers of the tiles are done
+  if (lane < nrow) rtab[lane] = make_float2(__int_as_float(jl), nl.x);
+  // whole rows of B: lane copies 16 bytes (4 columns) of rows 4i + lane/8
+#pragma unroll
+  for (int i = 0; i < kGroup / 4; ++i) {
+    const int r = 4 * i + (lane >> 3);
+    const int j = __shfl_sync(0xffffffffu, jl, r);
+    if (any_nd && r < nrow)
+      cp_async16(Bs + r * 32 + (lane & 7) * 4, brow + (size_t)j * kCol + (lane & 7) * 4);
+  }
+  for (int r = 0; r < nrow; ++r) {
+    const int j = __shfl_sync(0xffffffffu, jl, r);
+    if (nd && le.e0 >= 0) cp_async4(Cs + r * 32 + lane, cp0 + (size_t)j * nlag);
+  }
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncwarp();                       // every lane's rows of B have landed
+  // a column touched by further peaks applies them here in application
+  // order; otherwise its single peak is applied in the first pass below
+  const bool fused = rest_any == 0u;
+  if (!fused) {
+    if (nd && le.e0 >= 0) {
+      for (int r = 0; r < nrow; ++r)
+        Bs[r * 32 + lane] = __fsub_rn(Bs[r * 32 + lane], __fmul_rn(amp0, Cs[r * 32 + lane]));
+    }
+    for (unsigned m = rest_any; m; m &= m - 1u) {
+      const int e = __ffs(m) - 1;
+      const bool mine = nd && ((le.rest >> e) & 1u);
+      const float* cp = a.ctcT + (size_t)tl.k[e] * K * nlag + (c - tl.tau[e] + nt);
+      for (int r = 0; r < nrow; ++r) {
+        const int j = __shfl_sync(0xffffffffu, jl, r);
+        if (mine) cp_async4(Cs + r * 32 + lane, cp + (size_t)j * nlag);
+      }
+      cp_async_commit();
+      cp_async_wait_all();
+      if (mine) {
+        const float amp = tl.amp[e];
+        for (int r = 0; r < nrow; ++r)
+          Bs[r * 32 + lane] = __fsub_rn(Bs[r * 32 + lane], __fmul_rn(amp, Cs[r * 32 + lane]));
+      }
+    }
+  }
+  // pass 1: (single peak) subtraction, write-back, smallest exponent, and
+  // the largest approximate score; branch-free over all kGroup rows (rows
+  // past nrow and columns without nd only compute, their results unused)
+  float* bdst = a.Bt + (size_t)blk * K * kCol + lane;
+  const bool sub = fused && le.e0 >= 0;
+  float m = -1.f;
+  unsigned nanrows = 0u;
+  int emin = 255;
+#pragma unroll 8
+  for (int r = 0; r < kGroup; ++r) {
+    const int j = __shfl_sync(0xffffffffu, jl, r);
+    const float nmy = __shfl_sync(0xffffffffu, nl.y, r);
+    const bool ok = nd && r < nrow;
+    const float b0 = Bs[r * 32 + lane];
+    const float b1 = __fsub_rn(b0, __fmul_rn(amp0, Cs[r * 32 + lane]));
+    const float b = sub ? b1 : b0;
+    if (ok && sub) Bs[r * 32 + lane] = b;
+    if (ok && store) bdst[(size_t)j * kCol] = b;
+    emin = ok ? min(emin, noop_expo(b)) : emin;
+    const float rl = b > 0.f ? b : 0.f;
+    const float ap = __fmul_rn(__fmul_rn(rl, rl), nmy);
+    nanrows |= (ok && ap != ap) ? (1u << r) : 0u;
+    m = (ok && ap == ap) ? fmaxf(m, ap) : m;
+  }
+  // pass 2: the rows that can hold the best
+  const float thr = m >= 7.8886091e-31f ? m * 0.99999905f : -1.f;   // 2^-100
+  unsigned cand = nanrows;
+#pragma unroll 8
+  for (int r = 0; r < kGroup; ++r) {
+    const float nmy = __shfl_sync(0xffffffffu, nl.y, r);
+    const bool ok = nd && r < nrow;
+    const float b = Bs[r * 32 + lane];
+    const float rl = b > 0.f ? b : 0.f;
+    const float ap = __fmul_rn(__fmul_rn(rl, rl), nmy);
+    cand |= (ok && ap >= thr) ? (1u << r) : 0u;
+  }
+  // exact quotients of the candidates (usually one per column)
+  float best = -1.f;
+  int arg = 0x7fffffff;
+  for (unsigned mm = cand; mm; mm &= mm - 1u) {
+    const int r = __ffs(mm) - 1;
+    const float b = Bs[r * 32 + lane];
+    const float2 jn = rtab[r];
+    const int j = __float_as_int(jn.x);
+    const float rl = b > 0.f ? b : 0.f;
+    const float sq = __fmul_rn(rl, rl);
+    const bool normal = jn.y >= 1.17549435e-38f && jn.y <= 3.40282347e38f;
+    const float cf = (sq == 0.f && normal) ? 0.f : __fdiv_rn(sq, jn.y);
+    if (cf > best || (cf == best && j < arg)) {
+      best = cf;
+      arg = j;
+    }
+  }
+  unsigned long long gb = 0ull;
+  if (nd) {
+    gb = best >= 0.f ? pack_score(best, arg) : 0ull;
+    const size_t mi = ((size_t)blk * a.ng + g) * 32 + lane;
+    a.gbest[mi] = gb;
+    a.gexp[mi] = (unsigned char)emin;
+  }
+  return gb;
+}
+
+// Row indices and {nm, 1/nm} of group g, lane r holding position r.
+__device__ __forceinline__ void group_rows(const PeelArgs& a, int g, int lane, int& jl, float2& nl) {
+  const int rr = g * kGroup + lane;
+  jl = 0;
+  nl = make_float2(1.f, 1.f);
+  if (rr < a.K) {
+    jl = __ldg(a.rperm + rr);
+    nl = __ldg(a.nmip + rr);
+  }
+}
+
+// Initial scores of groups [g_lo, g_hi) of block blk (nothing subtracted):
+// every group's gbest and gexp, and the column maxima folded into pack_out.
+__device__ void group_init_item(const PeelArgs& a, const Smem& s, int blk, int g_lo, int g_hi,
+                                unsigned long long* pack_out, int lane, int warp) {
+  const int c = blk * kCol + lane;
+  const bool colok = c < a.L;
+  const TouchList none{0, nullptr, nullptr, nullptr};
+  const LaneEntries le{-1, 0u};
+  unsigned long long colbest = 0ull;
+  for (int g = g_lo; g < g_hi; ++g) {
+    int jl;
+    float2 nl;
+    group_rows(a, g, lane, jl, nl);
+    const unsigned long long gb = group_tile(a, s, none, blk, g, colok, le, false, jl, nl, lane, warp);
+    colbest = gb > colbest ? gb : colbest;
+  }
+  if (colok && colbest) atomicMax(&pack_out[c], colbest);
+}
+
+// Phase A for dirty block blk (iteration parity p): publish the block's
+// ordered touch list for its units, decide per column and group from the
+// metadata, fold the cached bests of the groups a column leaves alone (and
+// the settled score of a column no peak touches) into pack_out, and append
+// the groups some column must process to the unit list.
+__device__ void group_scan_block(const PeelArgs& a, const Smem& s, int p, int blk,
+                                 unsigned long long* pack_out, int lane, int warp) {
+  const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
+  int* bl = a.blist + (size_t)blk * 32;
+  if (lane == 0) bl[0] = tl.n;
+  if (lane < tl.n) {
+    bl[1 + lane] = tl.tau[lane];
+    bl[1 + kTouch + lane] = tl.k[lane];
+    bl[1 + 2 * kTouch + lane] = __float_as_int(tl.amp[lane]);
+  }
+  const int c = blk * kCol + lane;
+  const bool colok = c < a.L;
+  const int nt = a.nt, ng = a.ng;
+  unsigned tmask = 0u;
+  for (int e = 0; e < tl.n; ++e) {
+    const int d = c - tl.tau[e];
+    if (colok && d >= -nt && d <= nt) tmask |= 1u << e;
+  }
+  const bool touched = tmask != 0u;
+  const size_t meta = (size_t)blk * ng * 32 + lane;
+  unsigned char* eb = s.eb + warp * (kTouch * 32);
+  unsigned* ucount = a.wctr + 2 + p;
+  unsigned long long colbest = 0ull;
+  for (int gc = 0; gc < ng; gc += 32) {
+    const int gn = min(32, ng - gc);
+    const unsigned gmask = gn == 32 ? 0xffffffffu : ((1u << gn) - 1u);
+    // exponent fields of the product bounds of every touching peak, for the
+    // groups gc + lane
+    __syncwarp();
+    for (int e = 0; e < tl.n; ++e) {
+      int x = 255;
+      if (lane < gn)
+        x = bound_expo(__fmul_rn(fabsf(tl.amp[e]), __ldg(a.mg + (size_t)tl.k[e] * ng + gc + lane)));
+      eb[e * 32 + lane] = (unsigned char)x;
+    }
+    __syncwarp();
+    unsigned need = 0u;
+    if (touched) {
+#pragma unroll 8
+      for (int i = 0; i < gn; ++i) {
+        const int ex = a.gexp[meta + (size_t)(gc + i) * 32];
+        bool nd = false;
+        for (unsigned m = tmask; m; m &= m - 1u) {
+          const int e = __ffs(m) - 1;
+          nd |= (int)eb[e * 32 + i] + 26 > ex;
+        }
+        if (nd) need |= 1u << i;
+      }
+      const unsigned keep = ~need & gmask;
+#pragma unroll 8
+      for (int i = 0; i < gn; ++i) {
+        if ((keep >> i) & 1u) {
+          const unsigned long long gb = a.gbest[meta + (size_t)(gc + i) * 32];
+          colbest = gb > colbest ? gb : colbest;
+        }
+      }
+    }
+    const unsigned proc = __reduce_or_sync(0xffffffffu, need);
+    if (proc) {
+      unsigned base = 0u;
+      if (lane == 0) base = atomicAdd(ucount, (unsigned)__popc(proc));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      unsigned cols = 0u;             // lane i: the columns that process group gc + i
+      for (unsigned m = proc; m; m &= m - 1u) {
+        const int i = __ffs(m) - 1;
+        const unsigned b = __ballot_sync(0xffffffffu, (need >> i) & 1u);
+        if (lane == i) cols = b;
+      }
+      if ((proc >> lane) & 1u)
+        a.units[base + __popc(proc & ((1u << lane) - 1u))] =
+            make_uint2(((unsigned)blk << 11) | (unsigned)(gc + lane), cols);
+    }
+  }
+  if (colok) {
+    if (touched) {
+      if (colbest) atomicMax(&pack_out[c], colbest);
+    } else {
+      atomicMax(&pack_out[c], pack_score(a.cfmax[c], a.imax[c]));
+    }
+  }
+}
+
+// Phase B: one unit (a group tile that some columns of a block must
+// process), its block's ordered touch list read back from the scan.
+// unit_fetch issues the unit's loads (the block's list, the group's rows);
+// unit_run uses them, so a warp fetches its next unit before running the
+// current one.
+struct UnitFetch {
+  uint2 u;
+  int v;        // word `lane` of the block's list (n, tau[], k[], amp bits[])
+  int jl;       // row index of group position `lane`
+  float2 nl;    // its {nm, 1/nm}
+};
+
+__device__ __forceinline__ UnitFetch unit_fetch(const PeelArgs& a, uint2 u, int lane) {
+  UnitFetch f;
+  f.u = u;
+  const int blk = (int)(u.x >> 11), g = (int)(u.x & 2047u);
+  f.v = lane < 1 + 3 * kTouch ? a.blist[(size_t)blk * 32 + lane] : 0;
+  group_rows(a, g, lane, f.jl, f.nl);
+  return f;
+}
+
+__device__ void unit_run(const PeelArgs& a, const Smem& s, const UnitFetch& f,
+                         unsigned long long* pack_out, int lane, int warp) {
+  const int blk = (int)(f.u.x >> 11), g = (int)(f.u.x & 2047u);
+  const bool nd = (f.u.y >> lane) & 1u;
+  const int n = __shfl_sync(0xffffffffu, f.v, 0);
+  int* tau = s.tl_tau + warp * kTouch;
+  int* kk = s.tl_k + warp * kTouch;
+  float* amp = s.tl_amp + warp * kTouch;
+  const int tv = __shfl_sync(0xffffffffu, f.v, 1 + (lane & (kTouch - 1)));
+  const int kv = __shfl_sync(0xffffffffu, f.v, 1 + kTouch + (lane & (kTouch - 1)));
+  const int av = __shfl_sync(0xffffffffu, f.v, 1 + 2 * kTouch + (lane & (kTouch - 1)));
+  __syncwarp();
+  if (lane < n) {
+    tau[lane] = tv;
+    kk[lane] = kv;
+    amp[lane] = __int_as_float(av);
+  }
+  __syncwarp();
+  const TouchList tl{n, tau, kk, amp};
+  const int c = blk * kCol + lane;
+  const LaneEntries le = lane_entries(tl, c, c < a.L, a.nt);
+  const unsigned long long gb = group_tile(a, s, tl, blk, g, nd, le, true, f.jl, f.nl, lane, warp);
+  if (nd && gb) atomicMax(&pack_out[c], gb);
+}
+
 // Block of the rank-th set bit of the dirty bitmap (s.wprefix holds the
 // exclusive prefix of the word popcounts).
 __device__ __forceinline__ int dirty_block(const Smem& s, const unsigned* bits,
@@ -547,7 +963,7 @@ struct PeelOutcome {
 // (written by one thread) and is returned to every thread.  When the status
 // is KS_OK every record and residual list of the batch is complete and
 // visible to the team (the last pass ended at a team barrier).
-template <int kRows>
+template <int kRows, bool kGrouped>
 __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsigned G,
                                 unsigned& epoch) {
   const int tid = threadIdx.x;
@@ -569,7 +985,7 @@ __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsi
     for (long long i = t0; i < 2LL * a.nwords; i += ts) a.dbits[i] = 0u;
     for (long long i = t0; i < 2LL * a.L; i += ts) a.pack[i] = 0ull;
     for (long long i = t0; i < a.nblk; i += ts) a.xcount[i] = 0;
-    if (t0 < 2) a.wctr[t0] = 0u;
+    if (t0 < 6) a.wctr[t0] = 0u;
   }
   if (!ks_grid_sync(a.bar, G, epoch, a.err, a.limit_ns)) {
     const int e = ks_ld_volatile(a.err);
@@ -585,13 +1001,24 @@ __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsi
   // initial scores of every column, folded into pack[1]
   {
     unsigned long long* pinit = a.pack + (size_t)a.L;
-    const int rg = (a.K + kItemRows - 1) / kItemRows;
-    const TouchList none{0, nullptr, nullptr, nullptr};
-    const long long n_items = (long long)a.nblk * rg;
-    for (long long w = gwarp; w < n_items; w += nwarps) {
-      const int blk = (int)(w / rg), r = (int)(w % rg);
-      update_warp_item<kRows>(a, none, blk, r * kItemRows, min(a.K, (r + 1) * kItemRows), pinit,
-                              lane, true);
+    if (kGrouped) {
+      // items of kInitGroups groups: the group metadata of every column too
+      const int rg = (a.ng + kInitGroups - 1) / kInitGroups;
+      const long long n_items = (long long)a.nblk * rg;
+      for (long long w = gwarp; w < n_items; w += nwarps) {
+        const int blk = (int)(w / rg), r = (int)(w % rg);
+        group_init_item(a, s, blk, r * kInitGroups, min(a.ng, (r + 1) * kInitGroups), pinit,
+                        lane, warp);
+      }
+    } else {
+      const int rg = (a.K + kItemRows - 1) / kItemRows;
+      const TouchList none{0, nullptr, nullptr, nullptr};
+      const long long n_items = (long long)a.nblk * rg;
+      for (long long w = gwarp; w < n_items; w += nwarps) {
+        const int blk = (int)(w / rg), r = (int)(w % rg);
+        update_warp_item<kRows>(a, none, blk, r * kItemRows, min(a.K, (r + 1) * kItemRows),
+                                pinit, lane, true);
+      }
     }
   }
 
@@ -641,56 +1068,93 @@ __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsi
       a.tcount[(size_t)q * a.nblk + w] = 0;
     for (int w = rank * kThreads + tid; w < a.nwords; w += (int)G * kThreads)
       a.dbits[(size_t)q * a.nwords + w] = 0u;
-    if (rank == 0 && tid == 0) a.wctr[q] = 0u;
-    // update items: (dirty block in column order, row range), sized so that
-    // there are about four per warp
-    // rows per item: the split whose most loaded warp has the least work
-    // (row groups of 16 plus one group's worth of per-item set-up)
-    const int item_cap = nwarps >= kStaticWarps ? kItemRows : kItemRowsSmall;
-    int rows = kItemRows;
-    if (ndirty > 0) {
-      long long best_cost = -1;
-      for (int r = kRows; r <= item_cap; r += kRows) {
-        const long long items = (long long)ndirty * ((a.K + r - 1) / r);
-        const long long per_warp = (items + nwarps - 1) / nwarps;
-        const long long cost = per_warp * (r / kRows + 1);
-        if (best_cost < 0 || cost < best_cost) {
-          best_cost = cost;
-          rows = r;
-        }
-      }
+    if (rank == 0 && tid == 0) {
+      a.wctr[q] = 0u;
+      a.wctr[2 + q] = 0u;
+      a.wctr[4 + q] = 0u;
     }
-    const int rgroups = (a.K + rows - 1) / rows;
-    const long long n_upd = (long long)ndirty * rgroups;
-    const long long n_items = n_upd;
     if (rank == 0 && tid == 0) a.itoff[it] = (int)n_out;
     unsigned long long* pcur = a.pack + (size_t)p * a.L;
     KS_TRACE(it, 3, ks_globaltimer());
-    // Items go to warps in item order, so consecutive items (neighbouring
-    // blocks, which share the slabs of their peaks) run at about the same
-    // time.  A small team takes every item from the counter: warps that ran
-    // into slower memory take fewer of them (a static deal left the blocks
-    // of a 14-block team up to 20 % of an iteration apart at the closing
-    // barrier).  A large team deals all but its last round round-robin, so
-    // thousands of warps do not queue on one counter.
-    const long long rounds = n_items / nwarps;
-    const long long n_static =
-        (nwarps >= kStaticWarps && rounds > 1) ? (rounds - 1) * nwarps : 0;
-    for (long long w = gwarp; w < n_static; w += nwarps) {
-      const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
-      const int r = (int)(w % rgroups);
-      const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
-      update_warp_item<kRows>(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
-    }
-    while (true) {
-      unsigned next = 0;
-      if (lane == 0) next = atomicAdd(&a.wctr[p], 1u);
-      const long long w = n_static + (long long)__shfl_sync(0xffffffffu, next, 0);
-      if (w >= n_items) break;
-      const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
-      const int r = (int)(w % rgroups);
-      const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
-      update_warp_item<kRows>(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
+    if (kGrouped) {
+      // phase A: one warp per dirty block, dealt round-robin (metadata only,
+      // about the same work per block)
+      for (long long w = gwarp; w < ndirty; w += nwarps)
+        group_scan_block(a, s, p, dirty_block(s, bits, a.nwords, (int)w), pcur, lane, warp);
+      if (!ks_grid_sync(a.bar, G, epoch, a.err, a.limit_ns)) break;
+      // phase B: the units, taken from a counter in claims of about a quarter
+      // of a warp's share (at most 32), so thousands of warps do not queue on
+      // it; a warp reads its claim's records at once and fetches each unit's
+      // inputs while it runs the one before
+      const unsigned n_units = ks_ld_acquire(a.wctr + 2 + p);
+      const unsigned claim =
+          (unsigned)min(32LL, max(1LL, (long long)n_units / (nwarps * 4)));
+      while (true) {
+        unsigned first = 0;
+        if (lane == 0) first = atomicAdd(&a.wctr[4 + p], claim);
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (first >= n_units) break;
+        const int nu = (int)(min(n_units, first + claim) - first);
+        const uint2 rec = lane < nu ? a.units[first + lane] : make_uint2(0u, 0u);
+        UnitFetch cur = unit_fetch(
+            a, make_uint2(__shfl_sync(0xffffffffu, rec.x, 0), __shfl_sync(0xffffffffu, rec.y, 0)),
+            lane);
+        for (int i = 0; i < nu; ++i) {
+          UnitFetch nxt = cur;
+          if (i + 1 < nu)
+            nxt = unit_fetch(a, make_uint2(__shfl_sync(0xffffffffu, rec.x, i + 1),
+                                           __shfl_sync(0xffffffffu, rec.y, i + 1)),
+                             lane);
+          unit_run(a, s, cur, pcur, lane, warp);
+          cur = nxt;
+        }
+      }
+    } else {
+      // update items: (dirty block in column order, row range): the split
+      // whose most loaded warp has the least work (row steps of kRows plus one
+      // step's worth of per-item set-up)
+      const int item_cap = nwarps >= kStaticWarps ? kItemRows : kItemRowsSmall;
+      int rows = kItemRows;
+      if (ndirty > 0) {
+        long long best_cost = -1;
+        for (int r = kRows; r <= item_cap; r += kRows) {
+          const long long items = (long long)ndirty * ((a.K + r - 1) / r);
+          const long long per_warp = (items + nwarps - 1) / nwarps;
+          const long long cost = per_warp * (r / kRows + 1);
+          if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            rows = r;
+          }
+        }
+      }
+      const int rgroups = (a.K + rows - 1) / rows;
+      const long long n_items = (long long)ndirty * rgroups;
+      // Items go to warps in item order, so consecutive items (neighbouring
+      // blocks, which share the slabs of their peaks) run at about the same
+      // time.  A small team takes every item from the counter: warps that ran
+      // into slower memory take fewer of them (a static deal left the blocks
+      // of a 14-block team up to 20 % of an iteration apart at the closing
+      // barrier).  A large team deals all but its last round round-robin, so
+      // thousands of warps do not queue on one counter.
+      const long long rounds = n_items / nwarps;
+      const long long n_static =
+          (nwarps >= kStaticWarps && rounds > 1) ? (rounds - 1) * nwarps : 0;
+      for (long long w = gwarp; w < n_static; w += nwarps) {
+        const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
+        const int r = (int)(w % rgroups);
+        const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
+        update_warp_item<kRows>(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
+      }
+      while (true) {
+        unsigned next = 0;
+        if (lane == 0) next = atomicAdd(&a.wctr[p], 1u);
+        const long long w = n_static + (long long)__shfl_sync(0xffffffffu, next, 0);
+        if (w >= n_items) break;
+        const int blk = dirty_block(s, bits, a.nwords, (int)(w / rgroups));
+        const int r = (int)(w % rgroups);
+        const TouchList tl = load_touch_warp(a, s, p, blk, lane, warp);
+        update_warp_item<kRows>(a, tl, blk, r * rows, min(a.K, (r + 1) * rows), pcur, lane);
+      }
     }
     KS_TRACE(it, 4, ks_globaltimer());
     __syncthreads();
@@ -711,14 +1175,19 @@ __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsi
   return PeelOutcome{n_out, it, e ? e : status};
 }
 
+// kGrouped: the grouped update (a.rperm, a.nmip, a.mg and the group metadata
+// set); the ungrouped form needs no group metadata.
+template <bool kGrouped>
 __global__ void __launch_bounds__(kThreads, 2) peel_kernel(PeelArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
-  const Smem s = carve_smem(a, smem_raw);
+  const Smem s = carve_smem(a, smem_raw, kGrouped);
   unsigned epoch = 0;
-  run_peel<kRowsPerWarp>(a, s, blockIdx.x, gridDim.x, epoch);
+  run_peel<kRowsPerWarp, kGrouped>(a, s, blockIdx.x, gridDim.x, epoch);
 }
 
 constexpr int kXTile = kCol * (kCol + 1);   // floats of one warp's transpose tile
+// the batched peel's residual lists and transpose tiles fit in the stage tiles
+static_assert(3 * kXList * 4 + kXTile * 4 <= 2 * kGroup * 32 * 4, "residual scratch exceeds a stage tile");
 
 struct ResSmem {
   const float* W;  // Wt[t][8]: the basis transposed, components padded to 8
@@ -975,22 +1444,125 @@ __global__ void ks_ctc_transpose_kernel(const float* __restrict__ ctc, int K, in
   }
 }
 
+// ------------------------------------------------------------ group order
+// Setup of the grouped update.  The order only decides how many (column,
+// group) pairs the no-op test can leave alone; any order gives the same
+// results.
+//
+// Spatial key of each template: the channel centroid sum_c c*e_c / sum_c e_c
+// of its energy e_c = sum_p U[k,p,c]^2 (0 for a template without energy).
+// One warp per template, fixed summation order.
+__global__ void ks_template_key_kernel(const float* __restrict__ U, int K, int P, int C,
+                                       float* __restrict__ key) {
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= K) return;
+  double se = 0.0, sc = 0.0;
+  for (int c = lane; c < C; c += 32) {
+    float e = 0.f;
+    for (int p = 0; p < P; ++p) {
+      const float u = U[((size_t)w * P + p) * C + c];
+      e = fmaf(u, u, e);
+    }
+    se += e;
+    sc += (double)c * e;
+  }
+  for (int o = 16; o; o >>= 1) {
+    se += __shfl_xor_sync(0xffffffffu, se, o);
+    sc += __shfl_xor_sync(0xffffffffu, sc, o);
+  }
+  if (lane == 0) key[w] = se > 0.0 ? (float)(sc / se) : 0.f;
+}
+
+__device__ __forceinline__ unsigned sortable_key(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// rperm[r] = the template of rank r in ascending key order (the smaller
+// template index first on equal keys): each thread counts the keys below its
+// own, staged through shared memory 1024 at a time.
+__global__ void __launch_bounds__(256) ks_group_order_kernel(const float* __restrict__ key, int K,
+                                                             int* __restrict__ rperm) {
+  __shared__ unsigned sk[1024];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned mine = k < K ? sortable_key(key[k]) : 0u;
+  int rank = 0;
+  for (int j0 = 0; j0 < K; j0 += 1024) {
+    const int n = min(1024, K - j0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sk[i] = sortable_key(key[j0 + i]);
+    __syncthreads();
+    if (k < K)
+      for (int i = 0; i < n; ++i) {
+        const unsigned v = sk[i];
+        rank += (v < mine || (v == mine && j0 + i < k)) ? 1 : 0;
+      }
+  }
+  if (k < K) rperm[rank] = k;
+}
+
+// mg[k][g] = the largest |ctcT[k][j][l]| over the rows j of group g (rows
+// rperm[32g ..]) and all lags l, by the integer maximum of the magnitude bits
+// (so a NaN anywhere gives a NaN bound, which never passes the no-op test).
+// One block of 256 threads per (template, group).
+__global__ void __launch_bounds__(256) ks_group_bound_kernel(const float* __restrict__ ctcT,
+                                                             const int* __restrict__ rperm, int K,
+                                                             int nlag, int ng,
+                                                             float* __restrict__ mg) {
+  __shared__ unsigned wm[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long items = (long long)K * ng;
+  for (long long item = blockIdx.x; item < items; item += gridDim.x) {
+    const int k = (int)(item / ng), g = (int)(item % ng);
+    unsigned m = 0u;
+    for (int r = warp; r < kGroup; r += 8) {
+      const int rr = g * kGroup + r;
+      if (rr >= K) break;
+      const float* row = ctcT + ((size_t)k * K + rperm[rr]) * nlag;
+      for (int l = lane; l < nlag; l += 32) m = max(m, __float_as_uint(row[l]) & 0x7fffffffu);
+    }
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __syncthreads();
+    if (lane == 0) wm[warp] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned x = 0u;
+      for (int w = 0; w < 8; ++w) x = max(x, wm[w]);
+      mg[item] = __uint_as_float(x);
+    }
+  }
+}
+
+// nmip[r] = nmi[rperm[r]]: {nm, 1/nm} of the template rows in group order.
+__global__ void ks_group_nmi_kernel(const float2* __restrict__ nmi, const int* __restrict__ rperm,
+                                    int K, float2* __restrict__ nmip) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < K; r += gridDim.x * blockDim.x)
+    nmip[r] = nmi[rperm[r]];
+}
+
 // Scratch of one team (reused for every batch it processes), for batches of
-// up to L padded samples: [ctl 256 B: barrier count, error word] [cfmax L]
-// [imax L] [pack 2L] [chunk counts] [chunk buffers 4 x nchunks*kChunk]
-// [tcount 2 nblk] [touch 2 nblk*kTouch] [dbits 2 nwords] [work counters 2].
-// Only the control words need zeroing before a launch; the team clears the
-// rest per batch.
+// up to L padded samples and K templates: [ctl 256 B: barrier count, error
+// word] [cfmax L] [imax L] [pack 2L] [chunk counts] [chunk buffers 4 x
+// nchunks*kChunk] [tcount 2 nblk] [touch 2 nblk*kTouch] [dbits 2 nwords]
+// [work counters 6], and for the grouped update [gbest nblk*ng*32 u64]
+// [gexp nblk*ng*32 u8] [blist nblk*32 int] [units nblk*ng uint2] (K = 0:
+// none).  Only the control words need zeroing before a launch; the team
+// clears the rest per batch (the initial scoring writes every gbest and gexp
+// entry).
 struct TeamLayout {
   size_t cfmax, imax, pack, chunk_cnt, chunk_tau, chunk_k, chunk_amp, chunk_th, tcount,
-      touch, dbits, wctr, bytes;
+      touch, dbits, wctr, gbest, gexp, blist, units, bytes;
 };
 
 __host__ __device__ inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
-__host__ __device__ inline TeamLayout team_layout(long long L) {
+__host__ __device__ inline int n_groups(long long K) { return (int)((K + kGroup - 1) / kGroup); }
+
+__host__ __device__ inline TeamLayout team_layout(long long L, long long K) {
   const long long nchunks = (L + kChunk - 1) / kChunk, nblk = (L + kCol - 1) / kCol;
   const long long nwords = (nblk + 31) / 32;
+  const size_t meta = (size_t)nblk * n_groups(K) * 32;
   TeamLayout t;
   size_t o = 256;
   t.cfmax = o; o = al256(o + 4 * (size_t)L);
@@ -1004,7 +1576,11 @@ __host__ __device__ inline TeamLayout team_layout(long long L) {
   t.tcount = o; o = al256(o + 8 * (size_t)nblk);
   t.touch = o; o = al256(o + 2 * sizeof(Touch) * (size_t)nblk * kTouch);
   t.dbits = o; o = al256(o + 8 * (size_t)nwords);
-  t.wctr = o; o = al256(o + 8);
+  t.wctr = o; o = al256(o + 24);
+  t.gbest = o; o = al256(o + 8 * meta);
+  t.gexp = o; o = al256(o + meta);
+  t.blist = o; o = al256(o + (K > 0 ? 128 * (size_t)nblk : 0));
+  t.units = o; o = al256(o + 8 * (size_t)nblk * n_groups(K));
   t.bytes = o;
   return t;
 }
@@ -1026,9 +1602,11 @@ __host__ __device__ inline ListLayout list_layout(long long L) {
   return t;
 }
 
-// Point the scratch fields of a at a team region and a list region.
-__host__ __device__ inline void bind_scratch(PeelArgs& a, char* team, char* lists) {
-  const TeamLayout t = team_layout(a.L);
+// Point the scratch fields of a at a team region and a list region; with
+// grouped, also the group metadata (a.K must be set).
+__host__ __device__ inline void bind_scratch(PeelArgs& a, char* team, char* lists,
+                                             bool grouped) {
+  const TeamLayout t = team_layout(a.L, grouped ? a.K : 0);
   const ListLayout l = list_layout(a.L);
   a.bar = reinterpret_cast<unsigned*>(team);
   a.err = reinterpret_cast<int*>(team + 64);
@@ -1047,6 +1625,11 @@ __host__ __device__ inline void bind_scratch(PeelArgs& a, char* team, char* list
   a.itoff = reinterpret_cast<int*>(lists + l.itoff);
   a.xcount = reinterpret_cast<int*>(lists + l.xcount);
   a.xlist = reinterpret_cast<int*>(lists + l.xlist);
+  a.gbest = grouped ? reinterpret_cast<unsigned long long*>(team + t.gbest) : nullptr;
+  a.gexp = grouped ? reinterpret_cast<unsigned char*>(team + t.gexp) : nullptr;
+  a.blist = grouped ? reinterpret_cast<int*>(team + t.blist) : nullptr;
+  a.units = grouped ? reinterpret_cast<uint2*>(team + t.units) : nullptr;
+  a.ng = grouped ? n_groups(a.K) : 0;
   a.nchunks = (int)((a.L + kChunk - 1) / kChunk);
   a.nblk = (int)((a.L + kCol - 1) / kCol);
   a.nwords = (a.nblk + 31) / 32;

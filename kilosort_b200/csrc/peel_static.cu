@@ -9,13 +9,20 @@
 //
 // The array below is a file-scope __device__ object of kPeelStaticBytes
 // bytes (7 MiB); every GPU that loads the library holds one copy until the
-// process exits.  It covers batches of up to KS_PEEL_STATIC_MAX_L padded
-// samples; longer batches are rejected with KS_ERR_UNSUPPORTED.
+// process exits.  It holds the scratch of batches of up to
+// KS_PEEL_STATIC_MAX_L padded samples with up to KS_PEEL_STATIC_MAX_K
+// templates (shorter batches leave room for more templates); any shape whose
+// scratch does not fit is rejected with KS_ERR_UNSUPPORTED and a message.
+// This entry point runs the peel's ungrouped update, whose scratch does not
+// grow with the number of templates times the batch length.
 //
 // In host code the name of the array only stands for the device object; the
-// kernel needs its device address, which cudaGetSymbolAddress returns.  The
-// first call on each device looks that address up with the device current
-// (and caches it); make that first call before any stream capture.
+// kernel needs its device address, which cudaGetSymbolAddress returns.  A
+// call on a stream that is not being captured looks the address up again
+// with the device current (so a device whose context was reset gets the
+// address of its new image) and caches it; a call inside a stream capture
+// uses the cached address, so the first call on each device must come
+// before any capture.
 //
 // All calls share the array and it keeps the previous call's contents.  The
 // parts that must start at zero (barrier, counters, registration lists and
@@ -43,16 +50,25 @@ StaticScratch& static_scratch() {
   return s;
 }
 
-// Device address of the array on the current device (looked up once per device).
-int scratch_address(int device, void** out) {
+// Device address of the array on the current device: looked up again when
+// the stream is not capturing, the cached value inside a capture.
+int scratch_address(int device, cudaStream_t stream, void** out) {
   if (device < 0 || device >= 64) return ks::fail(KS_ERR_UNSUPPORTED, "ks_peel_static: device index out of range");
   StaticScratch& s = static_scratch();
   std::lock_guard<std::mutex> lock(s.mu);
-  if (!s.addr[device]) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cs = cudaStreamCaptureStatusActive;   // unknown: do not call into the runtime
+  }
+  if (cs == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_peel_scratch);
     if (e != cudaSuccess) return ks::cuda_fail(e, "cudaGetSymbolAddress(g_peel_scratch)");
     s.addr[device] = p;
+  } else if (!s.addr[device]) {
+    return ks::fail(KS_ERR_UNSUPPORTED,
+                    "ks_peel_static: the first call on a device must come before any stream capture");
   }
   *out = s.addr[device];
   return KS_OK;
@@ -70,16 +86,19 @@ extern "C" KS_API int ks_peel_static(float* Bt, float* Xres, const float* U, con
     return fail(KS_ERR_UNSUPPORTED,
                 "ks_peel_static: batch length must be 1.." + std::to_string(KS_PEEL_STATIC_MAX_L) +
                     " padded samples (the fixed scratch array is sized for that)");
-  const size_t need = peel_scratch_size(L, K);
+  const size_t need = peel_scratch_size(L, K, false);
   if (need > kPeelStaticBytes)
-    return fail(KS_ERR_UNSUPPORTED, "ks_peel_static: scratch for this batch exceeds the fixed array");
+    return fail(KS_ERR_UNSUPPORTED,
+                "ks_peel_static: the scratch of L=" + std::to_string(L) + ", K=" + std::to_string(K) +
+                    " exceeds the fixed array (" + std::to_string(KS_PEEL_STATIC_MAX_L) +
+                    " samples hold up to " + std::to_string(KS_PEEL_STATIC_MAX_K) + " templates)");
   DeviceInfo dev;
   int rc = device_info(&dev);
   if (rc) return rc;
   void* ws = nullptr;
-  rc = scratch_address(dev.device, &ws);
+  rc = scratch_address(dev.device, static_cast<cudaStream_t>(stream), &ws);
   if (rc) return rc;
   return launch_peel_tiled(Bt, Xres, U, W, ctcT, nm, C, L, K, P, nt, th2, max_peels, capacity, st,
                            amps, th_amps, info, ws, kPeelStaticBytes,
-                           static_cast<cudaStream_t>(stream), kWaitLimitNs, nullptr);
+                           static_cast<cudaStream_t>(stream), wait_limit_ns(), nullptr, false);
 }

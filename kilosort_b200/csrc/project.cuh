@@ -78,7 +78,17 @@ int gemm_bf16x3(const __nv_bfloat16* Uhi, const __nv_bfloat16* Ulo,
 
 // Peel on a tiled score matrix Bt [ceil(L/32)][K][32] and a transposed
 // cross-correlation ctcT[k][j][lag] = ctc[j][k][lag].
-size_t peel_scratch_size(int64_t L, int64_t K);
+// grouped: the update that skips exact no-op (column, template group) pairs
+// (scratch for its metadata and tables); otherwise every row of a touched
+// column is rewritten.
+size_t peel_scratch_size(int64_t L, int64_t K, bool grouped);
+// Tables of the grouped update for one template set (group order, bounds,
+// {nm, 1/nm} in group order), built on the stream by launch_group_setup.
+size_t group_tables_bytes(int64_t K);
+int launch_group_setup(const float* U, const float* ctcT, const float2* nmi, int64_t K,
+                       int64_t P, int64_t C, int64_t nt, void* tables, cudaStream_t stream);
+void group_tables(void* tables, int64_t K, const int** rperm, const float** mg,
+                  const float2** nmip);
 int64_t tiled_rows_floats(int64_t L, int64_t K);
 int launch_tile_rows(const float* B, int64_t ldb, int64_t K, int64_t L, float* Bt,
                      cudaStream_t stream);
@@ -94,6 +104,6 @@ int launch_peel_tiled(float* Bt, float* Xres, const float* U, const float* W,
                       int64_t P, int64_t nt, float th2, int64_t max_peels,
                       int64_t capacity, int64_t* st, float* amps, float* th_amps,
                       int64_t* info, void* ws, size_t ws_bytes, cudaStream_t stream,
-                      unsigned long long limit_ns, const int* upstream_err);
+                      unsigned long long limit_ns, const int* upstream_err, bool grouped);
 
 }  // namespace ks

@@ -120,3 +120,20 @@ def test_batched_workspace_query_and_argument_checks():
     assert lib.ks_match_batches_workspace_size(recs, 2, bats, 3, 7, 2) == 0
     rc = lib.ks_match_batches(recs, 2, bats, 3, _lib.KS_PROJ_BF16X3, 2, 1, None, 0, None, None)
     assert rc == _lib.KS_ERR_WORKSPACE
+
+
+def test_static_peel_limits_are_checked_before_the_device():
+    """ks_peel_static refuses, with a message, a batch longer than its fixed
+    array holds and, at that longest batch, more templates than the array
+    holds; both checks come before any device call."""
+    lib = _lib.load()
+    max_l, max_k = 131072, 56896
+    rc = lib.ks_peel_static(None, None, None, None, None, None, 4, max_l + 1, 2, 6, 61, 64.0,
+                            1, 1, None, None, None, None, None)
+    assert rc == _lib.KS_ERR_UNSUPPORTED
+    assert b"131072" in lib.ks_last_error()
+    rc = lib.ks_peel_static(None, None, None, None, None, None, 4, max_l, max_k + 1, 6, 61,
+                            64.0, 1, 1, None, None, None, None, None)
+    assert rc == _lib.KS_ERR_UNSUPPORTED
+    msg = lib.ks_last_error()
+    assert b"K=56897" in msg and b"56896" in msg

@@ -4,11 +4,13 @@ Such callers (an acquisition loop that may not call cudaMalloc on its hot
 path, a plugin that owns no device allocator) pass inputs and outputs only;
 the peel's scratch is a fixed array inside the library.  This test calls the
 entry point through the C ABI twice in a row and checks each result against
-the workspace-based ks_peel on the same inputs (identical kernels, so the
+the workspace-based ks_peel on the same inputs (both peels are exact, so the
 outputs must be identical; the tolerance of the other parity tests is met
 with equality).  The second call runs with the array still holding the first
-call's contents.  The file is collected last so that a run stopping at the
-first failure has run every other test; it also passes alone.
+call's contents.  A batch of the longest length the array holds runs too,
+and the shapes beyond the array are refused.  The file is collected last so
+that a run stopping at the first failure has run every other test; it also
+passes alone.
 """
 import numpy as np
 import pytest
@@ -22,8 +24,8 @@ pytestmark = pytest.mark.gpu
 DEV = torch.device("cuda:0")
 
 
-def _inputs(seed, n_templates, length):
-    rec = synth.make_recording(seed, n_chan=64, probe="np1", n_templates=n_templates,
+def _inputs(seed, n_templates, length, n_chan=64):
+    rec = synth.make_recording(seed, n_chan=n_chan, probe="np1", n_templates=n_templates,
                                batch_lengths=[length], rate_hz=(10.0, 30.0))
     U = torch.from_numpy(rec.U)
     W = torch.from_numpy(rec.wPCA)
@@ -84,6 +86,18 @@ def test_static_peel_matches_workspace_peel_twice(cuda_device):
             assert torch.equal(got[key], ref[key]), key
 
 
+def test_static_peel_holds_its_longest_batch(cuda_device):
+    # KS_PEEL_STATIC_MAX_L padded samples (131072) with a small template set
+    lib = _lib.load()
+    inp = _inputs(33, 24, 131072 - 2 * 61, n_chan=32)
+    assert inp["X"].shape[1] == 131072
+    ref = _run(lib, inp, static=False, cap=40000)
+    got = _run(lib, inp, static=True, cap=40000)
+    assert ref["n"] > 0 and got["n"] == ref["n"]
+    for key in ("st", "amps", "th", "Bt", "Xres"):
+        assert torch.equal(got[key], ref[key]), key
+
+
 def test_static_peel_rejects_batches_beyond_the_array(cuda_device):
     lib = _lib.load()
     too_long = 131072 + 1
@@ -91,3 +105,8 @@ def test_static_peel_rejects_batches_beyond_the_array(cuda_device):
                             1, 1, None, None, None, None, None)
     assert rc == _lib.KS_ERR_UNSUPPORTED
     assert b"131072" in lib.ks_last_error()
+    # at the longest batch, one template more than the array holds
+    rc = lib.ks_peel_static(None, None, None, None, None, None, 4, 131072, 56897, 6, 61, 64.0,
+                            1, 1, None, None, None, None, None)
+    assert rc == _lib.KS_ERR_UNSUPPORTED
+    assert b"56896" in lib.ks_last_error()
