@@ -645,10 +645,10 @@ __device__ __forceinline__ LaneEntries lane_entries(const TouchList& tl, int c, 
 // cf = fl(sq / nm) (sq and the quotient normal), a row whose approx is below
 // (1 - 2^-20) times the largest approx m of the group cannot reach the exact
 // quotient of the row holding m, so only the rows at or above that level
-// (and rows whose approx is NaN) have their exact quotient computed and
-// folded (larger score, then the smaller template index).  When m is below
-// 2^-100 every row takes the exact path (a zero sq with a normal nm has the
-// quotient +0 and needs no division).
+// have their exact quotient computed and folded (larger score, then the
+// smaller template index); rows with sq = 0 and a normal nm have the
+// quotient +0 exactly, and rows whose approx is NaN or tiny are folded
+// exactly too.
 __device__ unsigned long long group_tile(const PeelArgs& a, const Smem& s, const TouchList& tl,
                                          int blk, int g, bool nd, const LaneEntries& le,
                                          bool store, int jl, float2 nl, int lane, int warp) {
@@ -709,14 +709,19 @@ __device__ unsigned long long group_tile(const PeelArgs& a, const Smem& s, const
       }
     }
   }
-  // pass 1: (single peak) subtraction, write-back, smallest exponent, and
-  // the largest approximate score; branch-free over all kGroup rows (rows
-  // past nrow and columns without nd only compute, their results unused)
+  // pass 1, branch-free over all kGroup rows (rows past nrow and columns
+  // without nd only compute, their results unused): the (single peak)
+  // subtraction, the write-back, the smallest exponent, and for the best
+  // score the largest approx m with its first row rm, the largest approx m2
+  // of the other rows, the smallest row index whose score is exactly 0
+  // (sq = 0 and a normal nm), and the rows that need an exact quotient
+  // whatever m is (approx NaN, or below 2^-100 with sq > 0).
   float* bdst = a.Bt + (size_t)blk * K * kCol + lane;
   const bool sub = fused && le.e0 >= 0;
-  float m = -1.f;
-  unsigned nanrows = 0u;
-  int emin = 255;
+  constexpr float kTiny = 7.8886091e-31f;     // 2^-100
+  float m = -1.f, m2 = -1.f;
+  int rm = -1, jz = 0x7fffffff, emin = 255;
+  unsigned spec = 0u;
 #pragma unroll 8
   for (int r = 0; r < kGroup; ++r) {
     const int j = __shfl_sync(0xffffffffu, jl, r);
@@ -725,32 +730,54 @@ __device__ unsigned long long group_tile(const PeelArgs& a, const Smem& s, const
     const float b0 = Bs[r * 32 + lane];
     const float b1 = __fsub_rn(b0, __fmul_rn(amp0, Cs[r * 32 + lane]));
     const float b = sub ? b1 : b0;
-    if (ok && sub) Bs[r * 32 + lane] = b;
     if (ok && store) bdst[(size_t)j * kCol] = b;
     emin = ok ? min(emin, noop_expo(b)) : emin;
     const float rl = b > 0.f ? b : 0.f;
-    const float ap = __fmul_rn(__fmul_rn(rl, rl), nmy);
-    nanrows |= (ok && ap != ap) ? (1u << r) : 0u;
-    m = (ok && ap == ap) ? fmaxf(m, ap) : m;
+    const float sq = __fmul_rn(rl, rl);
+    const float ap = __fmul_rn(sq, nmy);
+    const bool big = ok && ap >= kTiny;
+    const bool top = big && ap > m;
+    m2 = top ? m : (big ? fmaxf(m2, ap) : m2);
+    rm = top ? r : rm;
+    m = top ? ap : m;
+    jz = (ok && sq == 0.f && nmy == nmy && j < jz) ? j : jz;
+    spec |= (ok && (ap != ap || (ap < kTiny && sq != 0.f))) ? (1u << r) : 0u;
   }
-  // pass 2: the rows that can hold the best
-  const float thr = m >= 7.8886091e-31f ? m * 0.99999905f : -1.f;   // 2^-100
-  unsigned cand = nanrows;
-#pragma unroll 8
-  for (int r = 0; r < kGroup; ++r) {
-    const float nmy = __shfl_sync(0xffffffffu, nl.y, r);
-    const bool ok = nd && r < nrow;
-    const float b = Bs[r * 32 + lane];
-    const float rl = b > 0.f ? b : 0.f;
-    const float ap = __fmul_rn(__fmul_rn(rl, rl), nmy);
-    cand |= (ok && ap >= thr) ? (1u << r) : 0u;
-  }
-  // exact quotients of the candidates (usually one per column)
+  // Candidates for the best: with m >= 2^-90 the rows whose approx is at
+  // least (1 - 2^-20) m -- only rm, unless m2 reaches that level; below
+  // 2^-90 every row with approx >= 2^-100.  Rows with a smaller approx
+  // cannot reach the exact quotient of rm (or 2^-100 and the zeros), so the
+  // result is that of folding every row.
+  const bool regime_a = m >= 8.0779356e-28f;  // 2^-90
+  const float thr = regime_a ? m * 0.99999905f : kTiny;
+  const bool scan = !regime_a || m2 >= thr;
   float best = -1.f;
   int arg = 0x7fffffff;
+  if (jz != 0x7fffffff) {
+    best = 0.f;
+    arg = jz;
+  }
+  unsigned cand = spec;
+  if (regime_a && !scan) cand |= 1u << rm;
+  if (__any_sync(0xffffffffu, nd && scan)) {
+#pragma unroll 8
+    for (int r = 0; r < kGroup; ++r) {
+      const float nmy = __shfl_sync(0xffffffffu, nl.y, r);
+      const bool ok = nd && scan && r < nrow;
+      const float b0 = Bs[r * 32 + lane];
+      const float b1 = __fsub_rn(b0, __fmul_rn(amp0, Cs[r * 32 + lane]));
+      const float b = sub ? b1 : b0;
+      const float rl = b > 0.f ? b : 0.f;
+      const float ap = __fmul_rn(__fmul_rn(rl, rl), nmy);
+      cand |= (ok && ap >= thr) ? (1u << r) : 0u;
+    }
+  }
+  // exact quotients of the candidates (usually only rm, converged)
+  if (!nd) cand = 0u;
   for (unsigned mm = cand; mm; mm &= mm - 1u) {
     const int r = __ffs(mm) - 1;
-    const float b = Bs[r * 32 + lane];
+    float b = Bs[r * 32 + lane];
+    if (sub) b = __fsub_rn(b, __fmul_rn(amp0, Cs[r * 32 + lane]));
     const float2 jn = rtab[r];
     const int j = __float_as_int(jn.x);
     const float rl = b > 0.f ? b : 0.f;
