@@ -43,12 +43,12 @@ NT = 61
 N_PCS = 6
 TH = 8.0
 CFG = 2
-# DRAM bytes (read + write) of one peel_kernel launch on a C=384/K=600/60000-sample
-# batch, from the ncu capture summarised in profiles/peel_kernel_c384_k600.txt
-PEEL_TRAFFIC_BYTES = 8.678e9
-# DRAM bytes of one peel_multi_kernel launch over 20 such batches (20 teams, one
-# group), per batch, from profiles/peel_multi_kernel_c384_k600_20batches.txt
-PEEL_MULTI_TRAFFIC_BYTES_PER_BATCH = 182.941e9 / 20
+# ncu summaries of the peel launches on this workload; each holds a line
+# "dram_bytes_per_batch: <bytes>" (dram__bytes_read.sum + dram__bytes_write.sum
+# of the captured launch divided by the batches it covers), read at run time so
+# the roofline's traffic comes from the capture committed beside the code
+PEEL_PROFILE = "peel_kernel_c384_k600.txt"
+PEEL_MULTI_PROFILE = "peel_multi_kernel_c384_k600_20batches.txt"
 WORKLOAD = ("Neuropixels-scale matching: C=384 (NP1-like), K=600 templates, 20 batches x "
             "60000 samples (+2*61 pad), nt=61, n_pcs=6, Th_learned=8, max_peels=100")
 
@@ -77,6 +77,52 @@ def parse():
                    help="np1 workload: 'TEAMS,GROUPS' of the batched form instead of the "
                         "autotuned schedule (for profiling a fixed launch)")
     return p.parse_args()
+
+
+def profile_traffic(name):
+    """DRAM bytes per batch from profiles/<name> (its dram_bytes_per_batch
+    line) and the file it came from, or (None, None) without such a line."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_batch:"):
+                    return float(line.split(":", 1)[1].split()[0]), "profiles/" + name
+    except OSError:
+        pass
+    return None, None
+
+
+def reference_gpu_batch(rec, b, dev, reps=3):
+    """The reference's run_matching op sequence on the GPU: the oracle, which
+    restates kilosort/template_matching.py:170-244 with the same torch ops, run
+    on CUDA tensors with TF32 off (cudnn and matmul), on batch b of rec: one
+    warm-up call, then the median of `reps` calls, each bracketed by CUDA
+    events with the device synchronised on both sides (the loop syncs the
+    host every iteration, as the reference does).  Returns ms per batch."""
+    from oracle import matching as om
+    flags = (torch.backends.cudnn.allow_tf32, torch.backends.cuda.matmul.allow_tf32)
+    torch.backends.cudnn.allow_tf32 = False
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        U = torch.from_numpy(rec.U).to(dev)
+        W = torch.from_numpy(rec.wPCA).to(dev)
+        X = torch.from_numpy(np.ascontiguousarray(rec.batch(b))).to(dev)
+        ops = dict(Th_learned=TH, nt=NT, max_peels=100, wPCA=W)
+        ctc = om.prepare_matching(ops, U)
+        times = []
+        for i in range(1 + reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            e0.record()
+            om.run_matching(ops, X, U, ctc)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            if i:
+                times.append(e0.elapsed_time(e1))
+        return statistics.median(times)
+    finally:
+        torch.backends.cudnn.allow_tf32, torch.backends.cuda.matmul.allow_tf32 = flags
 
 
 def peaks():
@@ -186,6 +232,12 @@ def reference_arm(args, rank):
         "e2e": {"value": v, "unit": "channel-samples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if torch.cuda.is_available():
+        ms = reference_gpu_batch(rec, 0, torch.device("cuda", 0))
+        line["reference_gpu"] = {"value": rec.n_chan * NT_BATCH / (ms * 1e-3),
+                                 "unit": "channel-samples/s", "ms_per_batch": ms,
+                                 "kind": "port on CUDA, TF32 off",
+                                 "sample": "batch 0, median of 3 after 1 warm-up"}
     print(json.dumps(line), flush=True)
 
 UNEVEN = ("three recordings (C/K = 96/150, 384/600, 384/1000), 200 padded batches with "
@@ -611,6 +663,22 @@ def main():
         ms_b, _ = timed(batched_step, "bf16x3_batched", sampler)
         results["bf16x3_batched"] = dict(ms=ms_b,
                                          spikes=sum(len(r[0]) for r in matcher.results()))
+        # the same batched form with the plain-FP32 projection (same schedule),
+        # so the split/FP32 ratio is also stated at equal execution shape
+        matcher32 = BatchedMatcher([mrec], [(L, 0)] * len(Xs), "fp32", teams=teams, graph=True,
+                                   groups=groups)
+        for dst, X in zip(matcher32.X, Xs):
+            dst.copy_(X)
+
+        def batched32_step(form, spikes):
+            matcher32.launch()
+            spikes.append(0)
+
+        ms_b32, _ = timed(batched32_step, "fp32_batched")
+        results["fp32_batched"] = dict(ms=ms_b32,
+                                       spikes=sum(len(r[0]) for r in matcher32.results()))
+        del matcher32
+        forms.append("fp32_batched")
         forms.append("bf16x3_batched")
         head = "bf16x3_batched"
 
@@ -692,25 +760,30 @@ def main():
     proj_tflops = flop_proj / (stage["project"] * 1e-3) / 1e12
     peel_gbs = bytes_peel / (stage["peel"] * 1e-3) / 1e9
     fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
-    traffic = PEEL_TRAFFIC_BYTES if (C, K, NT_BATCH) == (384, 600, 60000) else None
+    same_sizes = (C, K, NT_BATCH) == (384, 600, 60000)
+    tb_single, src_single = profile_traffic(PEEL_PROFILE) if same_sizes else (None, None)
+    tb_multi, src_multi = profile_traffic(PEEL_MULTI_PROFILE) if same_sizes else (None, None)
+    traffic = tb_single
     if batched_stage is not None and head == "bf16x3_batched":
-        # one peel_multi_kernel launch covers all batches of the step; its
-        # traffic is the ncu figure of that launch (20 batches), scaled by the
-        # batches when the step has another count (same sizes)
+        # one peel_multi_kernel launch covers all batches of the step and
+        # applies their residuals too, so its algorithmic bytes add the 8*C*L
+        # of X/Xres per batch; its traffic is the ncu figure per batch of the
+        # committed capture times the batches of this step (same sizes)
         t_b = batched_stage["peel"] * 1e-3
-        traffic_m = PEEL_MULTI_TRAFFIC_BYTES_PER_BATCH * nb if traffic else None
+        bytes_multi = bytes_peel + bytes_res
+        traffic_m = tb_multi * nb if tb_multi else None
         roof = {"kernel": "peel_multi_kernel", "bound": "hbm",
-                "achieved": bytes_peel / t_b / 1e9, "peak": hbm, "unit": "GB/s",
-                "frac": bytes_peel / t_b / 1e9 / hbm,
-                "traffic": traffic_m, "peak_source": peak_kind,
-                "algorithmic_bytes_per_launch": bytes_peel,
+                "achieved": bytes_multi / t_b / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": bytes_multi / t_b / 1e9 / hbm,
+                "traffic": traffic_m, "traffic_source": src_multi, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": bytes_multi,
                 "no_reuse_bytes_per_launch": bytes_noreuse,
                 "traffic_gbs": (traffic_m / t_b / 1e9 if traffic_m else None),
                 "ms_per_launch": batched_stage["peel"], "batches_per_launch": nb}
     elif stage["peel"] >= stage["project"]:
         roof = {"kernel": "peel_kernel", "bound": "hbm", "achieved": peel_gbs, "peak": hbm,
                 "unit": "GB/s", "frac": peel_gbs / hbm, "traffic": traffic,
-                "peak_source": peak_kind,
+                "traffic_source": src_single, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": bytes_peel / nb,
                 "no_reuse_bytes_per_launch": bytes_noreuse / nb,
                 "traffic_gbs": (traffic / (stage["peel"] / nb * 1e-3) / 1e9
@@ -726,13 +799,21 @@ def main():
                 "traffic": None, "peak_source": "nominal FP32 FMA"}
 
     cpu = None
+    ref_gpu = None
     agr = {}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         st_r, amps_r, dt = cpu_oracle_batch(rec, 0, threads)
         cpu = {"value": C * NT_BATCH / dt, "unit": "channel-samples/s", "cores": threads,
                "kind": "port", "sample": "batch 0 (C=384, 60000 samples), oracle run_matching"}
+        ms_ref = reference_gpu_batch(rec, 0, dev)
+        ref_gpu = {"value": C * NT_BATCH / (ms_ref * 1e-3), "unit": "channel-samples/s",
+                   "ms_per_batch": ms_ref, "kind": "port on CUDA, TF32 off",
+                   "sample": "batch 0, median of 3 after 1 warm-up",
+                   "speedup_batched_split": (ms_ref * nb) / results[head]["ms"]}
         for form in forms:
+            if form == "fp32_batched":
+                continue          # bit-identical to one fp32 run_matching per batch (tests)
             if form == "bf16x3_batched":
                 matcher.launch()
                 st, amps, _, _ = matcher.results()[0]
@@ -766,6 +847,9 @@ def main():
                                   if "bf16x3" in results else None),
         "speedup_batched_split_vs_fp32": (results["fp32"]["ms"] / results[head]["ms"]
                                           if head == "bf16x3_batched" else None),
+        "speedup_batched_split_vs_batched_fp32": (
+            results["fp32_batched"]["ms"] / results[head]["ms"]
+            if "fp32_batched" in results else None),
         "batched_teams": teams,
         "batched_groups": groups if matcher is not None else None,
         "stages_ms_per_step": stage,
@@ -782,6 +866,7 @@ def main():
                          "residual": {"achieved_gbs": bytes_res / (stage["residual"] * 1e-3) / 1e9,
                                       "algorithmic_bytes": bytes_res}},
         "cpu_baseline": cpu,
+        "reference_gpu": ref_gpu,
         "clocks": sampler.summary(),
         # batched head: energy, {nm, 1/nm}, reorder, a temporal projection per
         # batch, grouped contraction, peel, residual

@@ -12,8 +12,10 @@ Parity of this restatement is pinned against outputs of the reference itself
 inputs and stores their outputs; ``tests/test_oracle_golden.py`` asserts that
 this module reproduces them bit for bit in float32).
 
-Every function runs in the dtype of its inputs, so the same code gives the
-float64 oracle used for error statements.
+Every function runs in the dtype and on the device of its inputs, so the same
+code gives the float64 oracle used for error statements and, on CUDA tensors,
+the reference's own op sequence on the GPU (the benchmark's reference-on-GPU
+timing).
 """
 from __future__ import annotations
 
@@ -86,11 +88,12 @@ def peel(B, Xres, U, W, ctc, nm, Th, nt, max_peels, capacity=SPIKE_CAPACITY):
     Returns (st [N,2] int64, amps [N,1], th_amps [N,1], n_iterations).
     """
     dt = B.dtype
-    lags = torch.arange(-nt, nt + 1)
-    taps = torch.arange(-(nt // 2), nt // 2 + 1)
-    st = torch.zeros((capacity, 2), dtype=torch.int64)
-    amps = torch.zeros((capacity, 1), dtype=dt)
-    th_amps = torch.zeros((capacity, 1), dtype=dt)
+    dev = B.device          # the reference's buffers live on its device (:186-188)
+    lags = torch.arange(-nt, nt + 1, device=dev)
+    taps = torch.arange(-(nt // 2), nt // 2 + 1, device=dev)
+    st = torch.zeros((capacity, 2), dtype=torch.int64, device=dev)
+    amps = torch.zeros((capacity, 1), dtype=dt, device=dev)
+    th_amps = torch.zeros((capacity, 1), dtype=dt, device=dev)
     n = 0
     it = 0
     for it in range(max_peels):
