@@ -2,7 +2,7 @@
 
 Run from the repository root in a container that has the reference checkout:
 
-    python tests/golden/make_golden.py [path/to/reference]
+    python tests/golden/make_golden.py path/to/reference
 
 The reference package cannot be imported whole offline (its ``__init__``
 pulls in faiss and matplotlib), so a namespace stub is registered for
@@ -26,6 +26,15 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from kilosort_b200 import synth  # noqa: E402
+
+
+def reference_path():
+    """The reference checkout: the first argument, else $KS_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KS_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} PATH_TO_REFERENCE "
+                 "(or set KS_REFERENCE)")
+    return ref
 
 
 def load_reference(path):
@@ -120,7 +129,7 @@ def run_extract(tm):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = reference_path()
     torch.set_num_threads(max(1, os.cpu_count() or 1))
     tm = load_reference(ref)
     for name, (kw, Th, mp, store) in CASES.items():

@@ -2,7 +2,7 @@
 
 Run from the repository root in a container that has the reference checkout:
 
-    python tests/golden/make_golden_detect.py [path/to/reference]
+    python tests/golden/make_golden_detect.py path/to/reference
 
 Runs the reference's own ``spikedetect.run`` (kilosort/spikedetect.py:199-307:
 template centres, nearest channels and templates, size weights, then per
@@ -36,6 +36,15 @@ SETTINGS = dict(nearest_chans=10, nearest_templates=100, min_template_size=10,
                 templates_from_data=False)
 
 
+def reference_path():
+    """The reference checkout: the first argument, else $KS_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KS_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} PATH_TO_REFERENCE "
+                 "(or set KS_REFERENCE)")
+    return ref
+
+
 def load_reference(path):
     sys.modules["faiss"] = types.ModuleType("faiss")
     pkg = types.ModuleType("kilosort")
@@ -55,7 +64,7 @@ def make_ops(rec):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = reference_path()
     sd = load_reference(ref)
     rec = synth.make_recording(**SEED)
     ops = make_ops(rec)

@@ -3,7 +3,7 @@
 Run from the repository root in a container that has the reference checkout,
 after make_golden.py:
 
-    python tests/golden/make_golden_post.py [path/to/reference]
+    python tests/golden/make_golden_post.py path/to/reference
 
 Loads the golden `extract` case (tests/golden/golden_extract.npz, its
 recording regenerated from the stored seed), and runs the reference's
@@ -30,6 +30,15 @@ sys.path.insert(0, ROOT)
 from kilosort_b200 import synth  # noqa: E402
 
 
+def reference_path():
+    """The reference checkout: the first argument, else $KS_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KS_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} PATH_TO_REFERENCE "
+                 "(or set KS_REFERENCE)")
+    return ref
+
+
 def load_reference(path):
     pkg = types.ModuleType("kilosort")
     pkg.__path__ = [os.path.join(path, "kilosort")]
@@ -43,7 +52,7 @@ def load_reference(path):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = reference_path()
     post, tm, ccg = load_reference(ref)
     g = np.load(os.path.join(HERE, "golden_extract.npz"))
     rec = synth.make_recording(**ast.literal_eval(str(g["seed_kwargs"])))

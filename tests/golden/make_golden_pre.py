@@ -2,7 +2,7 @@
 
 Run from the repository root in a container that has the reference checkout:
 
-    python tests/golden/make_golden_pre.py [path/to/reference]
+    python tests/golden/make_golden_pre.py path/to/reference
 
 Builds seeded raw int16 batches (kilosort_b200.synth.raw_batch), padded as a
 batch is, and runs the reference's own ``BinaryFiltered.filter``
@@ -43,6 +43,15 @@ CASES = {
 }
 
 
+def reference_path():
+    """The reference checkout: the first argument, else $KS_REFERENCE."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KS_REFERENCE")
+    if not ref:
+        sys.exit(f"usage: python {os.path.basename(__file__)} PATH_TO_REFERENCE "
+                 "(or set KS_REFERENCE)")
+    return ref
+
+
 def load_reference(path):
     sys.modules["faiss"] = types.ModuleType("faiss")
     pkg = types.ModuleType("kilosort")
@@ -68,7 +77,7 @@ def sha(a):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = reference_path()
     kio, kpre = load_reference(ref)
     cpu = torch.device("cpu")
     hp = kpre.get_highpass_filter(30000, 300, device=cpu)
