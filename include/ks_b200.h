@@ -366,6 +366,29 @@ KS_API int ks_spike_positions(const float* tF, const int64_t* templ, const int64
                               void* stream);
 
 /*
+ * Duplicate-spike removal of the Phy export: spikes in index order, a spike
+ * kept (keep[s] = 1) when its time is at least dt after the last kept spike
+ * of the same cluster, the first spike of each cluster always kept (keep is
+ * uint8 [N]).  spike_times int64 [N], spike_clusters int32 [N] (any order of
+ * times).  Scratch: ks_remove_duplicates_workspace_size(N) bytes.
+ * Replaces kilosort/postprocessing.py:10-30 (remove_duplicates, called by
+ * kilosort/io.py:356-358).
+ */
+KS_API size_t ks_remove_duplicates_workspace_size(int64_t N);
+KS_API int ks_remove_duplicates(const int64_t* spike_times, const int32_t* spike_clusters,
+                                int64_t N, int64_t dt, uint8_t* keep, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
+/*
+ * Template waveforms of the Phy export, templates[k, t, c] = sum_p
+ * Wall[k, c, p] * W[p, t] (products rounded, then summed over p in order),
+ * Wall [K, C, P], W [P, nt] (wPCA), templates [K, nt, C], all f32.
+ * Replaces kilosort/io.py:383-385 (templates.npy).
+ */
+KS_API int ks_phy_templates(const float* Wall, const float* W, int64_t K, int64_t C, int64_t P,
+                            int64_t nt, float* templates, void* stream);
+
+/*
  * Stage timing of ks_run_matching, for profiling the public call as it runs
  * (no work is skipped or added).  While enabled on the calling host thread,
  * ks_run_matching records CUDA events at five points on its stream: start,

@@ -82,6 +82,9 @@ SIGNATURES = {
     "ks_trace_read": (_int, [_vp, _int]),
     "ks_match_batches_workspace_size": (_sz, [_vp, _i64, _vp, _i64, _int, _i64]),
     "ks_match_batches": (_int, [_vp, _i64, _vp, _i64, _int, _i64, _i64, _vp, _sz, _vp, _vp]),
+    "ks_remove_duplicates_workspace_size": (_sz, [_i64]),
+    "ks_remove_duplicates": (_int, [_vp, _vp, _i64, _i64, _vp, _vp, _sz, _vp]),
+    "ks_phy_templates": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp]),
 }
 
 KS_MAX_BATCHES = 256

@@ -9,9 +9,13 @@ TEST INFRASTRUCTURE ONLY.  Restates with the same PyTorch ops:
 * ``amplitudes`` -- kilosort/io.py:353: the 2-norm of each spike's features;
 * ``similarity`` -- kilosort/CCG.py:94-102: the maximum over lags of the
   cross-correlation of the unit-norm templates (UtU over channels, WtW the
-  flipped full cross-correlation of the wPCA rows).
+  flipped full cross-correlation of the wPCA rows);
+* ``remove_duplicates`` -- kilosort/postprocessing.py:10-30 (a per-spike loop
+  in index order, as the reference's numba function);
+* ``phy_templates`` -- kilosort/io.py:383-387 (templates.npy, templates_ind.npy).
 
-Pinned against tests/golden/golden_post.npz (the reference's own outputs).
+Pinned against tests/golden/golden_post.npz and tests/golden/golden_phy.npz
+(the reference's own outputs; the latter from its save_to_phy).
 """
 from __future__ import annotations
 
@@ -42,3 +46,30 @@ def similarity(Wall, W, nt=61):
     Wnorm = Wall / (1e-6 + mu)
     UtU = torch.einsum('ilk, jlm -> ijkm', Wnorm, Wnorm)
     return torch.einsum('ijkm, kml -> ijl', UtU, WtW).numpy().max(axis=-1)
+
+
+def remove_duplicates(spike_times, spike_clusters, dt=15):
+    """kilosort/postprocessing.py:10-30: spikes in index order; a spike is
+    kept when its time is at least dt after the last kept spike of its
+    cluster (the first spike of a cluster is kept).  Returns
+    (spike_times[keep], spike_clusters[keep], keep)."""
+    spike_times = np.asarray(spike_times, dtype=np.int64)
+    spike_clusters = np.asarray(spike_clusters, dtype=np.int32)
+    keep = np.zeros(spike_times.size, bool)
+    last = {}
+    for i in range(spike_times.size):
+        t, c = int(spike_times[i]), int(spike_clusters[i])
+        t0 = last.get(c, t - dt)
+        if t >= t0 + dt:
+            last[c] = t
+            keep[i] = True
+    return spike_times[keep], spike_clusters[keep], keep
+
+
+def phy_templates(Wall, W):
+    """kilosort/io.py:383-387: templates [K, nt, C] = the products
+    Wall[k, c, p] * W[p, t] summed over p, and templates_ind [K, C]."""
+    templates = (Wall.unsqueeze(-1).cpu() * W.cpu()).sum(axis=-2).numpy()
+    templates = templates.transpose(0, 2, 1)
+    ind = np.tile(np.arange(Wall.shape[1])[np.newaxis, :], (templates.shape[0], 1))
+    return templates, ind
