@@ -295,6 +295,44 @@ KS_API int ks_detect(const float* X, int64_t C, int64_t L, const float* wTEMP, i
                      size_t workspace_bytes, void* stream);
 
 /*
+ * Universal templates learned from data (templates_from_data).
+ * ks_snippets: on one padded batch X [C, L], the isolated single-channel
+ * peaks -- |X[c,t]| the maximum of |X| over channels c-4..c+4 and samples
+ * t-5..t+5 and above th, alone among the peaks of channels c-6..c+6 and
+ * samples t-30..t+30 (the reference's float32 mean-pool test), nt or more
+ * samples from both edges -- in (channel, sample) order, and their snippets
+ * clips[base + i, j] = X[c, t - twav_min + j] (j < nt) for base + i <
+ * capacity; count (device int32) receives the batch's number of peaks.
+ * Replaces kilosort/spikedetect.py:33-48 (extract_snippets).
+ * ks_snippet_gram: scales each of the n snippets [n, nt] to unit norm in
+ * place and writes G = sum_i x_i x_i^T [nt, nt] (double; nt <= 64), whose
+ * leading eigenvectors are the truncated-SVD basis of the snippets.
+ * Replaces the data side of kilosort/spikedetect.py:70-73 (TruncatedSVD).
+ * ks_kmeans_step / ks_kmeans_mindist / ks_kmeans_candidates: one Lloyd step
+ * (labels int32 [n] in/out, -1 before the first step; sums [k, d] double,
+ * counts [k] int64, stats {inertia, changed labels} double), and the distance
+ * and candidate-potential steps of k-means++ seeding, over X [n, d] f32
+ * (d, k <= 64).  Replace the data side of kilosort/spikedetect.py:78-85
+ * (KMeans).
+ */
+KS_API size_t ks_snippets_workspace_size(int64_t C, int64_t L);
+KS_API int ks_snippets(const float* X, int64_t C, int64_t L, int64_t nt, int64_t twav_min,
+                       float th, int64_t base, int64_t capacity, float* clips, int32_t* count,
+                       void* workspace, size_t workspace_bytes, void* stream);
+KS_API size_t ks_snippet_gram_workspace_size(int64_t n, int64_t nt);
+KS_API int ks_snippet_gram(float* clips, int64_t n, int64_t nt, double* G, void* workspace,
+                           size_t workspace_bytes, void* stream);
+KS_API size_t ks_kmeans_workspace_size(int64_t n, int64_t d, int64_t k);
+KS_API int ks_kmeans_step(const float* X, int64_t n, int64_t d, const float* centers, int64_t k,
+                          int32_t* labels, double* sums, int64_t* counts, double* stats,
+                          void* workspace, size_t workspace_bytes, void* stream);
+KS_API int ks_kmeans_mindist(const float* X, int64_t n, int64_t d, const float* c, int init,
+                             double* d2, void* stream);
+KS_API int ks_kmeans_candidates(const float* X, int64_t n, int64_t d, const float* cand,
+                                int64_t T, const double* d2, double* pots, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
+/*
  * Template similarity, sim[i, j] = max over lags l of
  *   sum_{k,m} (sum_c Wn[i,c,k] Wn[j,c,m]) * WtW[k,m,l],  Wn = Wall / (1e-6 + ||Wall||),
  * with WtW the flipped full cross-correlation of the wPCA rows (as ks_ctc).

@@ -85,6 +85,15 @@ SIGNATURES = {
     "ks_remove_duplicates_workspace_size": (_sz, [_i64]),
     "ks_remove_duplicates": (_int, [_vp, _vp, _i64, _i64, _vp, _vp, _sz, _vp]),
     "ks_phy_templates": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp]),
+    "ks_snippets_workspace_size": (_sz, [_i64, _i64]),
+    "ks_snippets": (_int, [_vp, _i64, _i64, _i64, _i64, _f32, _i64, _i64, _vp, _vp, _vp, _sz,
+                           _vp]),
+    "ks_snippet_gram_workspace_size": (_sz, [_i64, _i64]),
+    "ks_snippet_gram": (_int, [_vp, _i64, _i64, _vp, _vp, _sz, _vp]),
+    "ks_kmeans_workspace_size": (_sz, [_i64, _i64, _i64]),
+    "ks_kmeans_step": (_int, [_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "ks_kmeans_mindist": (_int, [_vp, _i64, _i64, _vp, _int, _vp, _vp]),
+    "ks_kmeans_candidates": (_int, [_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _sz, _vp]),
 }
 
 KS_MAX_BATCHES = 256

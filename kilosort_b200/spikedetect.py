@@ -10,13 +10,24 @@ sums over sizes and waveforms, the neighbourhood maximum, the max-pool and
 the peak test, the amplitudes, y positions and PC features -- is one call of
 ``ks_detect`` (no tensor of all the sums is ever stored).
 
-The universal waveforms and basis come from ``ops['wTEMP']``/``ops['wPCA']``
-(the reference's built-in templates file, or templates learned from data
-elsewhere); learning them here (``templates_from_data``: k-means and SVD of
-snippets) is not on the device path.
+The universal waveforms and basis come, as in the reference's ``run``
+(:205-216), either from its built-in templates file (``get_waves``, read from
+the same place the reference keeps its download, $KILOSORT_LOCAL_DOWNLOADS_PATH
+or ~/.kilosort; this build does not download it) or, with
+``settings['templates_from_data']``, from the data (``extract_wPCA_wTEMP``,
+:50-92): the isolated single-channel peaks of every 25th batch
+(``ks_snippets``), the exact truncated-SVD basis of their unit-norm snippets
+(``ks_snippet_gram`` on the device, the 61 x 61 symmetric eigenproblem on the
+host, rows signed as sklearn's TruncatedSVD signs them) and k-means of the
+snippets (k-means++ seeding and Lloyd steps on the device:
+``ks_kmeans_mindist``, ``ks_kmeans_candidates``, ``ks_kmeans_step``; ten
+seeded starts, the lowest inertia kept, as sklearn's KMeans with
+n_init=10).  The reference's TruncatedSVD and KMeans are randomized
+(random_state=None); these are deterministic for a given ``seed``.
 """
 from __future__ import annotations
 
+import os
 from typing import Optional
 
 import numpy as np
@@ -76,6 +87,181 @@ def geometry(ops, device=torch.device("cuda")):
     weigh = torch.permute(weigh, (2, 0, 1)).contiguous()
     weigh = weigh / (weigh ** 2).sum(1).unsqueeze(1) ** .5
     return iC, iC2, weigh
+
+
+def template_path(basename="wTEMP.npz"):
+    """Where the reference keeps its built-in universal templates
+    (kilosort/utils.py:22-38): $KILOSORT_LOCAL_DOWNLOADS_PATH, else
+    ~/.kilosort, file ``basename``."""
+    base = os.environ.get("KILOSORT_LOCAL_DOWNLOADS_PATH") or os.path.join(
+        os.path.expanduser("~"), ".kilosort")
+    return os.path.join(base, basename)
+
+
+def get_waves(ops, device=torch.device("cuda")):
+    """kilosort/spikedetect.py:94-98: (wPCA, wTEMP) of the built-in templates
+    file.  The reference downloads the file when it is missing; this build
+    has no download and raises FileNotFoundError instead."""
+    path = template_path()
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} not found: place the reference's wTEMP.npz there (or set "
+            "KILOSORT_LOCAL_DOWNLOADS_PATH), or set settings['templates_from_data']")
+    dd = np.load(path)
+    return (torch.from_numpy(dd["wPCA"]).to(device), torch.from_numpy(dd["wTEMP"]).to(device))
+
+
+def extract_snippets(X, nt, twav_min, Th_single_ch, device=None):
+    """Same inputs and output as kilosort/spikedetect.py:33-48: the snippets
+    [n, nt] of the isolated single-channel peaks of one padded batch X [C, L],
+    in (channel, sample) order, on the device (``ks_snippets``)."""
+    dev = torch.device(device) if device is not None else X.device
+    if dev.type != "cuda":
+        raise ValueError("snippets are extracted on a CUDA device (no CPU fallback)")
+    Xd = X.to(dev, torch.float32).contiguous()
+    C, L = Xd.shape
+    # isolated peaks are more than 6 channels or 30 samples apart: at most
+    # (C + 7) (L + 31) / (7 * 31) of them
+    cap = (C + 7) * (L + 31) // (7 * 31) + 1
+    clips = torch.empty((cap, nt), dtype=torch.float32, device=dev)
+    n = _snippets_into(Xd, nt, twav_min, Th_single_ch, clips, 0)
+    return clips[:n]
+
+
+def _snippets_into(Xd, nt, twav_min, th, clips, base):
+    """Snippets of one batch written at clips[base:]; returns the batch's count."""
+    lib = _lib.load()
+    C, L = Xd.shape
+    ws = torch.empty(lib.ks_snippets_workspace_size(C, L), dtype=torch.uint8, device=Xd.device)
+    count = torch.zeros(1, dtype=torch.int32, device=Xd.device)
+    _lib.check(lib.ks_snippets(_ptr(Xd), C, L, int(nt), int(twav_min), float(th), int(base),
+                               clips.shape[0], _ptr(clips), _ptr(count), _ptr(ws), ws.numel(),
+                               _stream(Xd.device)), "ks_snippets")
+    return int(count.item())
+
+
+def svd_basis(clips, n_pcs):
+    """The top ``n_pcs`` right singular vectors [n_pcs, nt] of the snippets
+    after each is scaled to unit norm (in place): the Gram matrix on the
+    device (``ks_snippet_gram``, double), its eigenvectors on the host in
+    descending eigenvalue order, each row signed so its largest-magnitude
+    entry is positive (sklearn's TruncatedSVD convention, which the
+    reference's wPCA follows).  float32 on the device of ``clips``."""
+    n, nt = clips.shape
+    dev = clips.device
+    lib = _lib.load()
+    G = torch.empty((nt, nt), dtype=torch.float64, device=dev)
+    ws = torch.empty(lib.ks_snippet_gram_workspace_size(n, nt), dtype=torch.uint8, device=dev)
+    _lib.check(lib.ks_snippet_gram(_ptr(clips), n, nt, _ptr(G), _ptr(ws), ws.numel(),
+                                   _stream(dev)), "ks_snippet_gram")
+    w, V = np.linalg.eigh(G.cpu().numpy())
+    comp = V[:, np.argsort(w)[::-1][:n_pcs]].T
+    sgn = np.sign(comp[np.arange(comp.shape[0]), np.abs(comp).argmax(1)])
+    sgn[sgn == 0] = 1.0
+    return torch.from_numpy((comp * sgn[:, None]).astype(np.float32)).to(dev)
+
+
+def kmeans(X, k, n_init=10, max_iter=300, tol=1e-4, seed=0):
+    """k-means of the rows of X [n, d] (float32, CUDA), as sklearn's KMeans
+    (k-means++ seeding with 2 + log(k) local trials, Lloyd steps until the
+    labels stop changing or the squared center shift is at most tol times
+    the mean per-feature variance, ``n_init`` starts, the lowest inertia
+    kept), with its random choices drawn from numpy's RandomState(seed).
+    Returns (centers [k, d] float32 on X's device, inertia)."""
+    n, d = X.shape
+    dev = X.device
+    lib = _lib.load()
+    stream = _stream(dev)
+    ws = torch.empty(lib.ks_kmeans_workspace_size(n, d, max(k, 1)), dtype=torch.uint8,
+                     device=dev)
+    if ws.numel() == 0:
+        raise ValueError("kmeans: need n >= 1 and d, k <= 64")
+    labels = torch.empty(n, dtype=torch.int32, device=dev)
+    sums = torch.empty((max(k, 1), d), dtype=torch.float64, device=dev)
+    counts = torch.empty(max(k, 1), dtype=torch.int64, device=dev)
+    stats = torch.empty(2, dtype=torch.float64, device=dev)
+
+    def step(centers):
+        labels_k = centers.shape[0]
+        _lib.check(lib.ks_kmeans_step(_ptr(X), n, d, _ptr(centers), labels_k, _ptr(labels),
+                                      _ptr(sums), _ptr(counts), _ptr(stats), _ptr(ws),
+                                      ws.numel(), stream), "ks_kmeans_step")
+        return (sums[:labels_k].cpu().numpy(), counts[:labels_k].cpu().numpy(),
+                stats.cpu().numpy())
+
+    # tolerance: tol x the mean per-feature variance (one step against the origin)
+    labels.fill_(-1)
+    s1, _, st1 = step(torch.zeros((1, d), dtype=torch.float32, device=dev))
+    tol_s = tol * (st1[0] / n - float((s1[0] / n) @ (s1[0] / n))) / d
+    rng = np.random.RandomState(seed)
+    d2 = torch.empty(n, dtype=torch.float64, device=dev)
+    pots = torch.empty(64, dtype=torch.float64, device=dev)
+    trials = 2 + int(np.log(k))
+    best = None
+    for _ in range(n_init):
+        # k-means++ seeding
+        first = int(rng.randint(n))
+        centers = [X[first].clone()]
+        _lib.check(lib.ks_kmeans_mindist(_ptr(X), n, d, _ptr(centers[0]), 1, _ptr(d2), stream),
+                   "ks_kmeans_mindist")
+        d2h = d2.cpu().numpy()
+        pot = float(d2h.sum())
+        for _c in range(1, k):
+            cand = np.searchsorted(np.cumsum(d2h), rng.uniform(size=trials) * pot)
+            cand = np.minimum(cand, n - 1)
+            cx = X[torch.from_numpy(cand).to(dev)].contiguous()
+            _lib.check(lib.ks_kmeans_candidates(_ptr(X), n, d, _ptr(cx), trials, _ptr(d2),
+                                                _ptr(pots), _ptr(ws), ws.numel(), stream),
+                       "ks_kmeans_candidates")
+            b = int(np.argmin(pots[:trials].cpu().numpy()))
+            centers.append(cx[b].clone())
+            _lib.check(lib.ks_kmeans_mindist(_ptr(X), n, d, _ptr(centers[-1]), 0, _ptr(d2),
+                                             stream), "ks_kmeans_mindist")
+            d2h = d2.cpu().numpy()
+            pot = float(d2h.sum())
+        C = torch.stack(centers).contiguous()
+        Ch = C.cpu().numpy().astype(np.float64)
+        labels.fill_(-1)
+        for _it in range(max_iter):
+            sm, cn, st = step(C)
+            new = np.where(cn[:, None] > 0, sm / np.maximum(cn, 1)[:, None], Ch)
+            shift = float(((new - Ch) ** 2).sum())
+            Ch = new
+            C = torch.from_numpy(Ch.astype(np.float32)).to(dev)
+            if st[1] == 0 or shift <= tol_s:
+                break
+        inertia = float(step(C)[2][0])
+        if best is None or inertia < best[1]:
+            best = (C, inertia)
+    return best
+
+
+def extract_wPCA_wTEMP(ops, bfile, nt=61, twav_min=20, Th_single_ch=6, nskip=25,
+                       device=torch.device("cuda"), seed=0):
+    """Same inputs and outputs as kilosort/spikedetect.py:50-92: the snippets
+    of the isolated peaks of batches 0, nskip, 2 nskip, ... (up to 500000;
+    the batch that would pass that is left out, and the reading stops), wPCA
+    [n_pcs, nt] = their truncated-SVD basis (``svd_basis``), wTEMP
+    [n_templates, nt] = their k-means centers (``kmeans``) scaled to unit
+    norm; both float32 on ``device``."""
+    dev = torch.device(device)
+    if dev.type != "cuda":
+        raise ValueError("templates are learned on a CUDA device (no CPU fallback)")
+    cap = 500000
+    clips = torch.empty((cap, nt), dtype=torch.float32, device=dev)
+    i = 0
+    for j in range(0, bfile.n_batches, nskip):
+        X = bfile.padded_batch_to_torch(j, ops).to(dev, torch.float32).contiguous()
+        nnew = _snippets_into(X, nt, twav_min, Th_single_ch, clips, i)
+        if i + nnew > cap:
+            break
+        i += nnew
+    clips = clips[:i].contiguous()
+    s = ops["settings"]
+    wPCA = svd_basis(clips, s["n_pcs"])
+    wTEMP, _ = kmeans(clips, s["n_templates"], n_init=10, seed=seed)
+    wTEMP = wTEMP / (wTEMP ** 2).sum(1).unsqueeze(1) ** .5
+    return wPCA, wTEMP
 
 
 class Detector:
@@ -148,12 +334,19 @@ def template_match(X, ops, iC, iC2, weigh, device=torch.device("cuda")):
 
 def run(ops, bfile, device=torch.device("cuda"), progress_bar=None, clear_cache=False,
         verbose=False):
-    """Same inputs and outputs as kilosort/spikedetect.py:199-307 with the
-    universal templates already in ops ('wTEMP', 'wPCA'): (st [n, 6] float64 --
-    time in s, y, amplitude, index, batch, position --, tF [n, nC, P], ops)."""
-    if "wTEMP" not in ops or "wPCA" not in ops:
-        raise ValueError("ops['wTEMP'] and ops['wPCA'] are needed (learning them is not on "
-                         "the device path)")
+    """Same inputs and outputs as kilosort/spikedetect.py:199-307: (st [n, 6]
+    float64 -- time in s, y, amplitude, index, batch, position --, tF
+    [n, nC, P], ops).  The universal templates ops['wPCA'], ops['wTEMP'] come
+    from the data when settings['templates_from_data'] is set
+    (extract_wPCA_wTEMP), else from the built-in templates file (get_waves),
+    as the reference sets them (:205-216)."""
+    s = ops["settings"]
+    if s.get("templates_from_data", True):
+        ops["wPCA"], ops["wTEMP"] = extract_wPCA_wTEMP(
+            ops, bfile, nt=ops["nt"], twav_min=ops["nt0min"], Th_single_ch=s["Th_single_ch"],
+            nskip=25, device=device)
+    else:
+        ops["wPCA"], ops["wTEMP"] = get_waves(ops, device=device)
     iC, iC2, weigh = geometry(ops, device=device)
     det = Detector(ops, iC, iC2, weigh, device)
     nt = ops["nt"]

@@ -18,14 +18,21 @@ PyTorch/numpy operations, in the same order:
   time, peaks above Th_universal;
 * ``yweighted`` -- :190-197;
 * ``run_batches`` -- the per-batch loop of ``run`` (:250-285): st (time in
-  seconds, y, amplitude, signed index, batch, position) and the PC features.
+  seconds, y, amplitude, signed index, batch, position) and the PC features;
+* ``extract_snippets`` -- :33-48, the isolated single-channel peaks and their
+  snippets (templates_from_data);
+* ``svd_basis`` -- the exact truncated-SVD basis of the unit-norm snippets
+  with sklearn's sign convention (the reference's TruncatedSVD, :72-73, is
+  randomized and approximates it).
 
-Pinned against tests/golden/golden_detect.npz (the reference's own run()).
+Pinned against tests/golden/golden_detect.npz and golden_learn.npz (the
+reference's own run() and extract_snippets).
 """
 from __future__ import annotations
 
 import numpy as np
 import torch
+import torch.nn.functional as F
 from torch.nn.functional import conv1d, max_pool1d
 
 
@@ -127,3 +134,34 @@ def run_batches(batches, wTEMP, wPCA, iC, iC2, weigh, yc, nt, nt0, Th_universal,
         sts.append(st)
         tFs.append(xfeat.transpose(0, 1).numpy())
     return np.concatenate(sts), np.concatenate(tFs)
+
+
+def extract_snippets(X, nt, twav_min, Th_single_ch, loc_range=(4, 5), long_range=(6, 30)):
+    """kilosort/spikedetect.py:33-48 with the same torch ops: isolated
+    single-channel peaks (max_pool2d window, avg_pool2d count times its area
+    equal to 1), zero within nt of both edges, snippets in nonzero order."""
+    Xabs = X.abs()
+    Xmax = F.max_pool2d(Xabs.unsqueeze(0), [2 * loc_range[0] + 1, 2 * loc_range[1] + 1],
+                        stride=[1, 1], padding=[loc_range[0], loc_range[1]])[0]
+    ispeak = torch.logical_and(Xmax == Xabs, Xabs > Th_single_ch).float()
+    area = (2 * long_range[0] + 1) * (2 * long_range[1] + 1)
+    ispeak_sum = F.avg_pool2d(ispeak.unsqueeze(0), [2 * long_range[0] + 1, 2 * long_range[1] + 1],
+                              stride=[1, 1], padding=[long_range[0], long_range[1]])[0] * area
+    is_peak_iso = (ispeak_sum == 1) * (ispeak == 1)
+    is_peak_iso[:, :nt] = 0
+    is_peak_iso[:, -nt:] = 0
+    xy = is_peak_iso.nonzero()
+    return X[xy[:, :1], xy[:, 1:2] - twav_min + torch.arange(nt)]
+
+
+def svd_basis(clips, n_pcs):
+    """The exact top right singular vectors [n_pcs, nt] (float64) of the
+    unit-norm snippets, each row signed so its largest-magnitude entry is
+    positive (the sign convention of sklearn's TruncatedSVD, which
+    kilosort/spikedetect.py:72-73 uses)."""
+    x = np.asarray(clips, dtype=np.float64)
+    x = x / np.sqrt((x ** 2).sum(1, keepdims=True))
+    _, _, vt = np.linalg.svd(x, full_matrices=False)
+    comp = vt[:n_pcs]
+    sgn = np.sign(comp[np.arange(comp.shape[0]), np.abs(comp).argmax(1)])
+    return comp * sgn[:, None]

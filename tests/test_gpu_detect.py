@@ -47,10 +47,15 @@ def _compare(st, tF, st_r, tF_r):
     return len(both)
 
 
-def test_run_matches_reference(cuda_device):
+def test_run_matches_reference(cuda_device, tmp_path, monkeypatch):
+    # the built-in templates branch (templates_from_data off): run() reads
+    # wTEMP.npz where the reference keeps its download
+    np.savez(tmp_path / "wTEMP.npz", wTEMP=G["wTEMP"], wPCA=G["wPCA"])
+    monkeypatch.setenv("KILOSORT_LOCAL_DOWNLOADS_PATH", str(tmp_path))
     rec = synth.make_recording(**ast.literal_eval(str(G["seed_kwargs"])))
-    ops = _ops(rec)
+    ops = mk.make_ops(rec)
     st, tF, ops = sd.run(ops, synth.SyntheticBinary(rec, device=DEV), device=DEV)
+    np.testing.assert_array_equal(ops["wTEMP"].cpu().numpy(), G["wTEMP"])
     np.testing.assert_array_equal(ops["iC"].cpu().numpy(), G["iC"])
     np.testing.assert_array_equal(ops["iC2"].cpu().numpy(), G["iC2"])
     assert _compare(st, tF, G["st"], G["tF"]) > 100
@@ -109,3 +114,10 @@ def test_zero_batch_has_no_spikes(cuda_device):
     xy, imax, amp, adist, yct, tF = sd.Detector(ops, iC, iC2, weigh, DEV)(X)
     assert len(xy) == len(imax) == len(amp) == len(yct) == len(tF) == 0
     assert adist.shape == (iC.shape[0], 0)
+
+
+def test_run_without_templates_file_raises(cuda_device, tmp_path, monkeypatch):
+    monkeypatch.setenv("KILOSORT_LOCAL_DOWNLOADS_PATH", str(tmp_path))
+    rec = synth.make_recording(**ast.literal_eval(str(G["seed_kwargs"])))
+    with pytest.raises(FileNotFoundError):
+        sd.run(mk.make_ops(rec), synth.SyntheticBinary(rec, device=DEV), device=DEV)
