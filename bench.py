@@ -16,6 +16,7 @@ of KS_BENCH_E2E_GROUP = 5 batches, copies and read-back beside the matching).
 
     python bench.py --workload uneven     # three recordings, 200 uneven batches
     python bench.py --workload adjoint    # reconstruction loss + adjoint
+    python bench.py --workload extract    # drop-in extract over an int16 filtered file
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -62,13 +63,14 @@ def parse():
     p.add_argument("--batches", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="np1",
-                   choices=["np1", "uneven", "adjoint", "stream", "detect"],
+                   choices=["np1", "uneven", "adjoint", "stream", "detect", "extract"],
                    help="np1: C=384/K=600, 20 equal batches (default); uneven: three "
                         "recordings, 200 batches of uneven length, batched launches; "
                         "adjoint: reconstruction loss + hand-written adjoint on one "
                         "C=384/K=600 batch with the matcher's spikes; stream: int16 host "
                         "stream -> whitening -> batched matcher, C=384/K=2000, with "
-                        "periodic template refinement")
+                        "periodic template refinement; extract: the drop-in extract over "
+                        "an int16 BinaryFiltered-style file, device batch filter")
     p.add_argument("--group", type=int, default=50,
                    help="uneven workload: batches per batched call (one graph each)")
     p.add_argument("--group-stream", type=int, default=4,
@@ -545,6 +547,115 @@ def stream_main(args, dev, rank, world):
         print(json.dumps(line), flush=True)
 
 
+EXTRACT = ("drop-in extract over a BinaryFiltered-style int16 file in host memory: 385 file "
+           "channels (384 mapped, NP1-like), K=600 templates, {nb} batches of 60000 samples, "
+           "the reference's batch filter on the device (mean, CAR median, 300 Hz high-pass, "
+           "whitening with one-block drift correction), split-BF16 projection, PC features")
+
+
+def extract_main(args, dev, rank, world):
+    """kb.extract over a synth.FilteredBinary: host int16 file -> sorted host arrays."""
+    import kilosort_b200 as kb
+    from kilosort_b200 import filtered, synth
+    from kilosort_b200.preprocess import highpass_filter
+    nb = args.batches if args.batches != 20 else 8
+    rec = synth.config_recording(CFG, n_batches=nb)
+    C, n_bin = rec.n_chan, rec.n_chan + 1
+    # raw = round(200 * whitened signal) + offsets, drifts, common mode and
+    # noise of sd 20 on every file channel; whitening eye / 200 undoes the gain
+    raw = synth.raw_recording(rec, n_bin, np.arange(C), seed=1102, gain=200.0)[:nb * NT_BATCH]
+    rng = np.random.default_rng(1103)
+    W = torch.eye(C) / 200.0
+    xc, yc = rec.xc.astype(np.float32), rec.yc.astype(np.float32)
+    pos = np.vstack((xc, yc)).T
+    d2 = ((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1)
+    Kxx = torch.from_numpy(np.exp(-d2 / (2 * 20.0 ** 2)))
+    iKxx = torch.linalg.inv(Kxx + 0.01 * torch.eye(C)).to(dev)
+    ops = dict(Th_learned=TH, nt=NT, max_peels=100, wPCA=torch.from_numpy(rec.wPCA).to(dev),
+               nt0min=20, batch_size=NT_BATCH, xc=xc, yc=yc, nblocks=1,
+               yblk=np.array([yc.mean()]), probe=dict(xc=xc, yc=yc), iKxx=iKxx,
+               settings=dict(nearest_chans=10, position_limit=100, n_pcs=N_PCS, sig_interp=20.0))
+    src = synth.FilteredBinary(raw, NT=NT_BATCH, nt=NT, chan_map=np.arange(C),
+                               hp_filter=highpass_filter(), whiten_mat=W,
+                               dshift=rng.uniform(-5.0, 5.0, (nb, 1)), device=dev)
+    assert src.n_batches == nb and filtered.supports(src)
+    U = torch.from_numpy(rec.U).to(dev)
+    for _ in range(max(1, args.warmup)):
+        kb.extract(dict(ops), src, U, device=dev)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev.index or 0)
+    sampler.__enter__()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st, tF, _ = kb.extract(dict(ops), src, U, device=dev)
+    dt = (time.perf_counter() - t0) / args.steps
+    sampler.__exit__()
+    # the stages alone, one after the other: the batch source, then matching
+    fb = filtered.FilteredBatches(src, dev)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    Xs = [fb.batch(b, ops) for b in range(nb)]
+    fb.check()
+    t_src = time.perf_counter() - t1
+    fb.close()
+    ctc = kb.prepare_matching(ops, U)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    for X in Xs:
+        kb.run_matching(ops, X, U, ctc, device=dev)
+    torch.cuda.synchronize()
+    t_match = time.perf_counter() - t2
+    value = C * nb * NT_BATCH * world / dt
+    L = NT_BATCH + 2 * NT
+    line = {
+        "metric": "channel-samples/s", "value": value, "unit": "channel-samples/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int16 in, f32 (f32 filter, split-bf16 whitening and projection)",
+        "data": "synthetic",
+        "config": {"workload": EXTRACT.format(nb=nb), "batches": nb,
+                   "timing": "host wall clock around extract (host int16 file in, sorted "
+                             "st and tF on the host out)",
+                   "parallelism": f"replicas x{world}"},
+        "spikes_per_step": len(st),
+        "stages_ms": {"batch_source_alone": t_src * 1e3, "matching_alone": t_match * 1e3},
+        # per batch: filter 6, matching 7, features 1; per call: template
+        # channels, ctc (2), transpose
+        "gpu_launches": 14 * nb + 4,
+        "e2e": {"value": value, "unit": "channel-samples/s",
+                "h2d_bytes_per_step": nb * L * n_bin * 2,
+                "d2h_bytes_per_step": int(st.nbytes + tF.numel() * 4)},
+        "clocks": sampler.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the same extract fed the reference's way: the file slice transposed,
+        # a pageable copy, float32, and the torch filter (FFT high-pass) on the
+        # device -- the oracle's restatement of io.py:789-831 and :990-1026
+        from oracle import preprocess as op
+
+        class ReferenceRead(synth.FilteredBinary):
+            def padded_batch_to_torch(self, ibatch, ops=None):
+                return op.filtered_batch(self, ibatch, ops, self.device)
+
+        ref = ReferenceRead(raw, NT=NT_BATCH, nt=NT, chan_map=np.arange(C),
+                            hp_filter=src.hp_filter, whiten_mat=W, dshift=src.dshift, device=dev)
+        ops_r = dict(ops, device_filter=False)
+        kb.extract(dict(ops_r), ref, U, device=dev)
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        reps = max(1, min(3, args.steps))
+        for _ in range(reps):
+            st_r, _, _ = kb.extract(dict(ops_r), ref, U, device=dev)
+        dt_r = (time.perf_counter() - t3) / reps
+        line["reference_batch_source"] = {
+            "value": C * nb * NT_BATCH / dt_r, "unit": "channel-samples/s",
+            "ms_per_step": dt_r * 1e3, "spikes_per_step": len(st_r),
+            "kind": "port on CUDA (pageable float32 copy, torch FFT filter)",
+            "speedup_device_source": dt_r / dt}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -561,9 +672,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
 
-    if args.workload in ("uneven", "adjoint", "stream", "detect"):
+    if args.workload in ("uneven", "adjoint", "stream", "detect", "extract"):
         {"uneven": uneven_main, "adjoint": adjoint_main, "stream": stream_main,
-         "detect": detect_main}[args.workload](args, dev, rank, world)
+         "detect": detect_main, "extract": extract_main}[args.workload](args, dev, rank, world)
         if world > 1:
             dist.destroy_process_group()
         return

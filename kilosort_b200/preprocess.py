@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .template_matching import _stream
+from .template_matching import _stream, to_host
 
 
 def _ptr(t) -> int:
@@ -128,7 +128,7 @@ class Preprocessor:
 
     def status(self):
         """(device status, artifact) of the last call (synchronises)."""
-        f = self.flags.cpu().tolist()
+        f = to_host(self.flags)[0].tolist()
         return int(f[0]), bool(f[1])
 
 

@@ -43,6 +43,8 @@ __all__ = [
     "make_recording",
     "config_recording",
     "CONFIGS",
+    "raw_recording",
+    "FilteredBinary",
 ]
 
 
@@ -344,3 +346,96 @@ def raw_batch(seed: int, n_chan_bin: int, L: int, fs: float = 30000.0,
                 lo, hi = max(0, s - 15), min(L, s + 16)
                 x[lo:hi, cc] -= a * g * w[lo - (s - 15):hi - (s - 15)]
     return np.clip(np.round(x), -32768, 32767).astype(np.int16)
+
+
+def raw_recording(rec: Recording, n_chan_bin: int, chan_map, seed: int, gain: float = 25.0,
+                  fs: float = 30000.0, chunk: int = 65536) -> np.ndarray:
+    """The whole of ``rec`` as a raw int16 file ``[T, n_chan_bin]``.
+
+    Every file channel carries what preprocessing removes (as in `raw_batch`,
+    but continuous over the recording: a per-channel offset, a slow sinusoidal
+    drift, a common-mode 50 Hz signal with noise, white noise of sd 20); the
+    channels ``chan_map`` (in order) add ``round(gain * rec.signal)``, so a
+    whitening matrix ``eye / gain`` brings the signal back to its scale.
+    Generated in chunks of ``chunk`` samples in float32.
+    """
+    chan_map = np.asarray(chan_map)
+    if len(chan_map) != rec.n_chan:
+        raise ValueError("chan_map must name one file channel per recording channel")
+    T = rec.signal.shape[1]
+    rng = np.random.default_rng(seed)
+    off = rng.uniform(-500, 500, n_chan_bin).astype(np.float32)
+    f_drift = rng.uniform(1, 8, n_chan_bin)
+    a_drift = rng.uniform(20, 120, n_chan_bin).astype(np.float32)
+    ph = rng.uniform(0, 2 * np.pi, n_chan_bin)
+    out = np.empty((T, n_chan_bin), np.int16)
+    for s in range(0, T, chunk):
+        e = min(T, s + chunk)
+        t = np.arange(s, e) / fs
+        x = np.sin(2 * np.pi * f_drift[None, :] * t[:, None] + ph[None, :]).astype(np.float32)
+        x *= a_drift
+        x += off
+        common = 60 * np.sin(2 * np.pi * 50 * t) + 15 * rng.standard_normal(e - s)
+        x += common.astype(np.float32)[:, None]
+        x += 20 * rng.standard_normal((e - s, n_chan_bin), dtype=np.float32)
+        x[:, chan_map] += gain * rec.signal[:, s:e].T
+        np.clip(np.round(x), -32768, 32767, out=x)
+        out[s:e] = x
+    return out
+
+
+class FilteredBinary:
+    """An in-memory stand-in for the reference's ``BinaryFiltered``
+    (kilosort/io.py:968-1045) over a raw int16 (or uint16) array
+    ``[T, n_chan_bin]``, with ``tmin = 0``, ``tmax = inf``, no scale or shift.
+
+    It has the members a ``BinaryFiltered`` carries and `extract` reads:
+    ``file``, ``NT``, ``nt``, ``n_chan_bin``, ``dtype``, the filter settings
+    (``chan_map``, ``hp_filter``, ``whiten_mat``, ``dshift``, ``do_CAR``,
+    ``invert_sign``, ``artifact_threshold``), ``imin``/``imax``,
+    ``n_batches``, ``batch_downsampling`` and ``_get_batch_edges``, with the
+    batch count and edges of io.py:646-656 and :771-787: ``ceil(T / NT)``
+    batches, the last one dropped (and ``imax`` cut back) when it would hold
+    fewer than ``nt`` samples past its left pad; batch 0 covers
+    ``[imin, imin + NT + nt)``, batch b ``[imin + b NT - nt,
+    min(imax, imin + (b+1) NT + nt))``.  ``padded_batch_to_torch`` filters on
+    the device (``filtered.FilteredBatches``).
+    """
+
+    def __init__(self, data: np.ndarray, NT: int = 60000, nt: int = 61, chan_map=None,
+                 hp_filter=None, whiten_mat=None, dshift=None, do_CAR: bool = True,
+                 invert_sign: bool = False, artifact_threshold: float = np.inf,
+                 batch_downsampling: int = 1, device="cuda"):
+        self.file = data
+        self.dtype = str(data.dtype)
+        self.NT, self.nt = int(NT), int(nt)
+        self.n_chan_bin = int(data.shape[1])
+        self.chan_map, self.hp_filter, self.whiten_mat = chan_map, hp_filter, whiten_mat
+        self.dshift, self.do_CAR, self.invert_sign = dshift, do_CAR, invert_sign
+        self.artifact_threshold = artifact_threshold
+        self.scale = self.shift = None
+        self.device = device
+        self.imin, self.imax = 0, int(data.shape[0])
+        self.n_batches_raw = int(np.ceil((self.imax - self.imin) / self.NT))
+        a, b = self._get_batch_edges(self.n_batches_raw - 1)
+        tail = b - a - self.nt
+        if tail < self.nt:
+            self.n_batches_raw -= 1
+            self.imax -= tail
+        self.batch_downsampling = int(batch_downsampling)
+        self.n_batches = int(self.n_batches_raw / self.batch_downsampling)
+        self._device_batches = None
+
+    def _get_batch_edges(self, ibatch: int):
+        if ibatch == 0:
+            return self.imin, self.imin + self.NT + self.nt
+        start = self.imin + int(ibatch) * self.NT - self.nt
+        return start, min(self.imax, start + self.NT + 2 * self.nt)
+
+    def padded_batch_to_torch(self, ibatch: int, ops=None):
+        from .filtered import FilteredBatches
+        if self._device_batches is None:
+            self._device_batches = FilteredBatches(self, self.device, copy_threads=1)
+        X = self._device_batches.batch(ibatch, ops)
+        self._device_batches.check()
+        return X

@@ -23,6 +23,7 @@ one (default True; set False for a batch source whose
 from __future__ import annotations
 
 import logging
+import threading
 import weakref
 
 import numpy as np
@@ -89,6 +90,59 @@ class _Workspace:
 
 
 _ws = _Workspace()
+
+
+class _HostStage:
+    """Device->host reads through pinned staging.
+
+    The copies are queued (non-blocking) on the current stream of the
+    tensors' device into one pinned buffer per host thread, and waited for
+    with a CUDA event, which does not hold the GIL.  A pageable copy would
+    wait for the stream in the driver instead, and a host thread that waits
+    there for a long peel stalls the other threads' copies and launches (the
+    batch reader of `extract` filters the next batch meanwhile).  Returns
+    numpy copies, so the buffer is free again when `fetch` returns.
+    """
+
+    def __init__(self):
+        self._local = threading.local()
+
+    def _buffer(self, nbytes: int) -> torch.Tensor:
+        buf = getattr(self._local, "buf", None)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(max(4096, int(nbytes * 1.25)), dtype=torch.uint8, pin_memory=True)
+            self._local.buf = buf
+        return buf
+
+    def fetch(self, *tensors: torch.Tensor):
+        ts = [t.detach().contiguous() for t in tensors]
+        dev = next((t.device for t in ts if t.is_cuda), None)
+        if dev is None:                       # host tensors (the CPU checks of the loop)
+            return [t.numpy().copy() for t in ts]
+        offs, total = [], 0
+        for t in ts:
+            offs.append(total)
+            total += -(-t.numel() * t.element_size() // 64) * 64
+        buf = self._buffer(total)
+        views = []
+        for t, o in zip(ts, offs):
+            nb = t.numel() * t.element_size()
+            v = buf[o:o + nb].view(t.dtype).view(t.shape)
+            if nb:
+                v.copy_(t, non_blocking=True)
+            views.append(v)
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(dev))
+        ev.synchronize()
+        return [v.numpy().copy() for v in views]
+
+
+_host = _HostStage()
+
+
+def to_host(*tensors: torch.Tensor):
+    """numpy copies of device tensors, read through pinned staging (`_HostStage`)."""
+    return _host.fetch(*tensors)
 
 
 class _TransposedCtc:
@@ -177,7 +231,7 @@ def project_scores(X, U, W, nt, projection="fp32", tiled=False, check_status=Tru
 
 
 def _info_status(info, what):
-    n, status, iters, need = (int(v) for v in info.tolist())
+    n, status, iters, need = (int(v) for v in to_host(info)[0].tolist())
     if status == _lib.KS_ERR_OVERFLOW:
         raise RuntimeError(
             f"{what}: {need} spikes in one batch exceed the spike buffer "
@@ -361,9 +415,18 @@ def _match_features(ops, W, iCCd, iU, Ucc):
 
 
 class _BatchReader:
-    """Reads ``bfile.padded_batch_to_torch`` one batch ahead on a worker
-    thread, so the next batch's file read and host->device copy overlap the
-    current batch's matching.
+    """Reads padded batches one ahead on a worker thread, so the next batch's
+    file read, host->device copy and filter overlap the current batch's
+    matching.
+
+    A reference ``BinaryFiltered`` with int16 or uint16 samples (and no
+    scale or shift) on a CUDA device is read through
+    ``filtered.FilteredBatches``: the raw window goes into pinned memory,
+    crosses as int16 and is filtered on the device by ``ks_preprocess_int16``
+    -- the batch ``bfile.padded_batch_to_torch(ibatch, ops)`` returns
+    (kilosort/io.py:1037-1045), made on the device.  ``ops['device_filter'] =
+    False`` keeps the file's own ``padded_batch_to_torch``; any other source
+    uses it too.
 
     On a CUDA device the read runs on the reader's own stream and is complete
     when handed over (the stream is synchronised in the worker); the tensor is
@@ -376,21 +439,33 @@ class _BatchReader:
         self.device = torch.device(device) if device is not None else None
         self.pool = None
         self.next = None
+        self.streams = {}
+        self.filtered = None
+        from . import filtered          # imports this module's stream helper
+        if self.device is not None and self.device.type == "cuda" \
+                and ops.get("device_filter", True) and filtered.supports(bfile):
+            self.filtered = filtered.FilteredBatches(bfile, self.device)
         if ahead and len(self.order) > 1:
             from concurrent.futures import ThreadPoolExecutor
             self.pool = ThreadPoolExecutor(1, thread_name_prefix="ks-batch-reader")
-            self.streams = {}
             self.next = self.pool.submit(self._read, self.order[0])
+
+    def _load(self, ibatch):
+        if self.filtered is None:
+            return self.bfile.padded_batch_to_torch(ibatch, self.ops)
+        X = self.filtered.batch(ibatch, self.ops)
+        self.filtered.check()
+        return X
 
     def _read(self, ibatch):
         dev = self.device
         if self.pool is None or dev is None or dev.type != "cuda":
-            return self.bfile.padded_batch_to_torch(ibatch, self.ops)
+            return self._load(ibatch)
         if dev not in self.streams:
             self.streams[dev] = torch.cuda.Stream(dev)
         s = self.streams[dev]
         with torch.cuda.device(dev), torch.cuda.stream(s):
-            X = self.bfile.padded_batch_to_torch(ibatch, self.ops)
+            X = self._load(ibatch)
         s.synchronize()
         return X
 
@@ -411,6 +486,9 @@ class _BatchReader:
                 self.next.cancel()
             self.pool.shutdown(wait=True)
             self.pool = None
+        if self.filtered is not None:
+            self.filtered.close()
+            self.filtered = None
 
 
 def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=None,
@@ -456,13 +534,14 @@ def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=N
                 amps = amps[~neg, :]
                 th_amps = th_amps[~neg, :]
             t_shift = ibatch * bfile.batch_downsampling * (ops["batch_size"])
-            stt = stt.double()
-            rows = np.empty((len(stt), 3), "float64")
-            rows[:, 0] = ((stt[:, 0] - nt) + t_shift).cpu().numpy() - nt // 2 + ops["nt0min"]
-            rows[:, 1] = stt[:, 1].cpu().numpy()
-            rows[:, 2] = th_amps.cpu().numpy().squeeze(-1)
+            st_h, th_h, tf_h = to_host(stt, th_amps, xfeat)
+            # float64 as the reference computes them (exact for sample indices)
+            rows = np.empty((len(st_h), 3), "float64")
+            rows[:, 0] = ((st_h[:, 0].astype("float64") - nt) + t_shift) - nt // 2 + ops["nt0min"]
+            rows[:, 1] = st_h[:, 1]
+            rows[:, 2] = th_h.reshape(-1)
             sts.append(rows)
-            tFs.append(xfeat.cpu())
+            tFs.append(torch.from_numpy(tf_h))
             if progress_bar is not None:
                 progress_bar.emit(int((ibatch + 1) / bfile.n_batches * 100))
     except Exception:

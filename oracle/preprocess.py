@@ -13,7 +13,15 @@ same order:
   (lower median over channels), Fourier-domain high-pass with the half-length
   shift, artifact zeroing, whitening (drift matrix folded in as M @ Wrot);
 * ``drift_matrix`` -- kilosort/preprocessing.py:44-69 with one block
-  (kernel2D_torch, datashift.py:176-179; iKxx as datashift.py:216-223).
+  (kernel2D_torch, datashift.py:176-179; iKxx as datashift.py:216-223);
+* ``drift_matrix_ops`` -- kilosort/preprocessing.py:44-69 as the filter calls
+  it, from ``ops`` (blocks, their depths, probe, ``iKxx``, ``sig_interp``);
+* ``padded_batch`` -- kilosort/io.py:789-831 (BinaryRWFile.padded_batch_to_torch):
+  the file slice transposed, copied to the device as it is (pageable), made
+  float32 (uint16 shifted by 2**15), its edges repeated for the first and last
+  batch;
+* ``filtered_batch`` -- kilosort/io.py:1037-1045: ``padded_batch`` then
+  ``filter_batch`` with the batch's drift matrix.
 
 Pinned against tests/golden/golden_pre.npz (the reference's own filter run on
 the same inputs, tests/golden/make_golden_pre.py).
@@ -38,7 +46,7 @@ def fft_highpass(hp, n):
     ft = hp.shape[0]
     if ft < n:
         pad = (n - ft) // 2
-        z = lambda k: torch.zeros(k, dtype=hp.dtype)
+        z = lambda k: torch.zeros(k, dtype=hp.dtype, device=hp.device)
         return fft(torch.cat((z(pad), hp, z(pad + (n - pad * 2 - ft)))))
     if ft > n:
         crop = (ft - n) // 2
@@ -81,6 +89,21 @@ def drift_matrix(xc, yc, shift, sig_interp=20.0):
     yp[:, 1] -= shift
     Kyx = kernel2d(torch.from_numpy(yp), torch.from_numpy(xp), sig_interp)
     return Kyx @ iKxx
+
+
+def drift_matrix_ops(ops, dshift, device):
+    if ops["nblocks"] == 1:
+        shifts = dshift
+    else:
+        from scipy.interpolate import interp1d
+        f = interp1d(ops["yblk"], dshift, fill_value="extrapolate", kind="linear")
+        shifts = f(ops["probe"]["yc"])
+    xp = np.vstack((ops["probe"]["xc"], ops["probe"]["yc"])).T
+    yp = xp.copy()
+    yp[:, 1] -= shifts
+    Kyx = kernel2d(torch.from_numpy(yp).to(device), torch.from_numpy(xp).to(device),
+                   ops["settings"]["sig_interp"])
+    return Kyx @ ops["iKxx"].to(device)
 
 
 def centre_offset(ft, L):
@@ -138,3 +161,36 @@ def filter_batch_taps(X, taps, centre=None, chan_map=None, invert_sign=False, do
             W = drift.double() @ W
         X = W @ X
     return X
+
+
+def padded_batch(bfile, ibatch, device):
+    ibatch = int(ibatch) * bfile.batch_downsampling
+    bstart, bend = bfile._get_batch_edges(ibatch)
+    data = bfile.file[bstart:bend].T
+    if str(data.dtype) == "uint16":
+        data = data.astype("float32") - 2 ** 15
+    nsamp = data.shape[-1]
+    nt = bfile.nt
+    X = torch.zeros((bfile.n_chan_bin, bfile.NT + 2 * nt), device=device)
+    if ibatch == 0:
+        X[:, nt:nt + nsamp] = torch.from_numpy(data).to(device).float()
+        X[:, :nt] = X[:, nt:nt + 1]
+    elif ibatch == bfile.n_batches - 1:
+        X[:, :nsamp] = torch.from_numpy(data).to(device).float()
+        X[:, nsamp:] = X[:, nsamp - 1:nsamp]
+    else:
+        X[:] = torch.from_numpy(data).to(device).float()
+    return X
+
+
+def filtered_batch(bfile, ibatch, ops, device):
+    X = padded_batch(bfile, ibatch, device)
+    drift = None
+    if bfile.whiten_mat is not None and bfile.dshift is not None and ops is not None:
+        drift = drift_matrix_ops(ops, bfile.dshift[ibatch], device)
+    cmap = None if bfile.chan_map is None else torch.as_tensor(bfile.chan_map, device=device)
+    hp = None if bfile.hp_filter is None else bfile.hp_filter.to(device)
+    W = None if bfile.whiten_mat is None else bfile.whiten_mat.to(device)
+    return filter_batch(X, chan_map=cmap, invert_sign=bfile.invert_sign, do_car=bfile.do_CAR,
+                        hp=hp, artifact_threshold=bfile.artifact_threshold, whiten=W,
+                        drift=drift)
