@@ -21,11 +21,17 @@
 //                       per-sample lower median by a warp radix select on the
 //                       order-preserving integer keys of the floats, coalesced
 //                       [C][L] rows out
-//   ks_pre_fir_kernel   FP32 circular FIR, tiles of 128 samples x 16 channels,
-//                       8 samples per thread, taps in groups of 8 over a
-//                       16-sample register window; writes f32 rows, or the bf16
-//                       hi/lo samples-by-channels operand of the whitening
-//                       contraction; flags artifacts
+//                       (with a high-pass: the bf16 hi/lo samples of the
+//                       circularly padded batch P[c][j] = x[c][(j - h) mod L]
+//                       instead, the operand of the tensor-core FIR)
+//   fir_tc              with a high-pass: the FIR as a split-BF16 tcgen05
+//                       product with the Toeplitz matrix of the taps
+//                       (fir_tc.cu); writes f32 rows or the whitening operand,
+//                       flags artifacts
+//   ks_pre_fir_kernel   without one: the identity in the same output forms
+//                       (an FP32 circular FIR, tiles of 128 samples x 16
+//                       channels, 8 samples per thread, taps in groups of 8
+//                       over a 16-sample register window)
 //   whitening           the split-BF16 tcgen05 contraction (gemm_bf16x3)
 #include "ks_common.cuh"
 #include "project.cuh"
@@ -121,12 +127,16 @@ __device__ float warp_select(const float* tile, int pitch, int C, int s, int k, 
   return key_value(prefix);
 }
 
-// Centred (and common-average-referenced) samples: Xc[c][t], t < L.
-template <bool kCar>
+// Centred (and common-average-referenced) samples: Xc[c][t], t < L; with kPad
+// instead the bf16 hi/lo planes of the circularly padded batch
+// P[c][j] = x[c][(j - h) mod L], j < cols (sample t at every j = t + h mod L).
+template <bool kCar, bool kPad>
 __global__ void __launch_bounds__(kCarThreads)
 ks_pre_car_kernel(const int16_t* __restrict__ raw, int L, long long ldr,
                   const long long* __restrict__ map, int C, float sign,
-                  const double* __restrict__ sums, float* __restrict__ Xc, int* err) {
+                  const double* __restrict__ sums, float* __restrict__ Xc,
+                  __nv_bfloat16* __restrict__ Phi, __nv_bfloat16* __restrict__ Plo, int h,
+                  long long cols, int* err) {
   extern __shared__ __align__(16) float sm[];
   constexpr int pitch = kCarTile + 1;
   float* tile = sm;                                        // [C][pitch]
@@ -159,7 +169,17 @@ ks_pre_car_kernel(const int16_t* __restrict__ raw, int L, long long ldr,
     const int c = e / kCarTile, s = e - c * kCarTile;
     if (s < nt) {
       const float v = tile[c * pitch + s];
-      Xc[(size_t)c * L + t0 + s] = kCar ? __fsub_rn(v, med[s]) : v;
+      const float y = kCar ? __fsub_rn(v, med[s]) : v;
+      if (kPad) {
+        const __nv_bfloat16 hv = __float2bfloat16_rn(y);
+        const __nv_bfloat16 lv = __float2bfloat16_rn(y - __bfloat162float(hv));
+        for (long long j = (t0 + s + h) % L; j < cols; j += L) {
+          Phi[(size_t)c * cols + j] = hv;
+          Plo[(size_t)c * cols + j] = lv;
+        }
+      } else {
+        Xc[(size_t)c * L + t0 + s] = y;
+      }
     }
   }
 }
@@ -279,8 +299,8 @@ __global__ void ks_pre_zero_kernel(float* X, int C, int L, long long ldx, const 
 }
 
 struct PreLayout {
-  int64_t Cq, Cpad, Tpad;
-  size_t flags, sums, xc, whi, wlo, yhi, ylo, bytes;
+  int64_t Cq, Cpad, Tpad, pcols;
+  size_t flags, sums, xc, phi, plo, thi, tlo, whi, wlo, yhi, ylo, bytes;
 };
 
 PreLayout pre_layout(int64_t L, int64_t C, bool whiten) {
@@ -288,6 +308,8 @@ PreLayout pre_layout(int64_t L, int64_t C, bool whiten) {
   p.Cq = ks::round_up(C, 64);
   p.Cpad = ks::round_up(C, 128);
   p.Tpad = ks::round_up(L, 256);
+  // the padded FIR operand for the most taps and the longest output
+  p.pcols = ks::fir_tc_cols(whiten ? p.Tpad : L, kMaxTaps);
   size_t o = 0;
   auto take = [&](size_t b) {
     const size_t at = o;
@@ -297,6 +319,10 @@ PreLayout pre_layout(int64_t L, int64_t C, bool whiten) {
   p.flags = take(256);                     // [0] device error, [1] artifact
   p.sums = take(sizeof(double) * (size_t)C);
   p.xc = take(sizeof(float) * (size_t)C * L);
+  p.phi = take(2 * (size_t)C * p.pcols);
+  p.plo = take(2 * (size_t)C * p.pcols);
+  p.thi = take(ks::fir_tc_toeplitz_bytes(kMaxTaps) / 2);
+  p.tlo = take(ks::fir_tc_toeplitz_bytes(kMaxTaps) / 2);
   if (whiten) {
     p.whi = take(2 * (size_t)p.Cpad * p.Cq);
     p.wlo = take(2 * (size_t)p.Cpad * p.Cq);
@@ -349,56 +375,66 @@ extern "C" KS_API int ks_preprocess_int16(const int16_t* raw, int64_t L, int64_t
     ks_pre_sum_kernel<<<grid, 256, 0, s>>>(raw, (int)L, ld_raw, map, (int)C, chunk, sums, err);
     KS_CUDA(cudaGetLastError());
   }
-  // 2. centring and common average reference
+  // 2. centring and common average reference (with a high-pass: into the
+  //    padded bf16 operand of the tensor-core FIR)
+  const bool split = whiten != nullptr;
+  const int64_t rows = split ? p.Tpad : L;
+  const int64_t pcols = hp_taps ? ks::fir_tc_cols(rows, (int)ntaps) : 0;
+  __nv_bfloat16* phi = reinterpret_cast<__nv_bfloat16*>(base + p.phi);
+  __nv_bfloat16* plo = reinterpret_cast<__nv_bfloat16*>(base + p.plo);
   {
     const size_t smem = sizeof(float) * (size_t)C * (kCarTile + 1) + sizeof(int) * 8 * 256 +
                         sizeof(float) * kCarTile;
     const unsigned grid = (unsigned)((L + kCarTile - 1) / kCarTile);
     const float sign = invert_sign ? -1.f : 1.f;
-    if (do_car) {
-      KS_CUDA(cudaFuncSetAttribute(ks_pre_car_kernel<true>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      ks_pre_car_kernel<true><<<grid, kCarThreads, smem, s>>>(raw, (int)L, ld_raw, map, (int)C,
-                                                              sign, sums, Xc, err);
-    } else {
-      KS_CUDA(cudaFuncSetAttribute(ks_pre_car_kernel<false>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      ks_pre_car_kernel<false><<<grid, kCarThreads, smem, s>>>(raw, (int)L, ld_raw, map, (int)C,
-                                                               sign, sums, Xc, err);
-    }
-    KS_CUDA(cudaGetLastError());
+    auto run = [&](auto kernel) -> int {
+      KS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      kernel<<<grid, kCarThreads, smem, s>>>(raw, (int)L, ld_raw, map, (int)C, sign, sums, Xc,
+                                             phi, plo, (int)hp_centre, (long long)pcols, err);
+      KS_CUDA(cudaGetLastError());
+      return KS_OK;
+    };
+    int rc;
+    if (hp_taps)
+      rc = do_car ? run(ks_pre_car_kernel<true, true>) : run(ks_pre_car_kernel<false, true>);
+    else
+      rc = do_car ? run(ks_pre_car_kernel<true, false>) : run(ks_pre_car_kernel<false, false>);
+    if (rc) return rc;
   }
   // 3. high-pass (the identity when there is no filter), artifact flag
-  const float* taps = hp_taps;
-  const int nt = hp_taps ? (int)ntaps : 1;
-  const int centre = hp_taps ? (int)hp_centre : 0;
   const bool check = artifact_threshold < INFINITY;
   {
-    const bool split = whiten != nullptr;
-    // the split operand is written whole (Tpad rows, zeros past L)
-    const int tiles_t = (int)(((split ? p.Tpad : L) + kFirT - 1) / kFirT);
-    const int cgroups = (int)((split ? p.Cq : C) + kFirC - 1) / kFirC;
-    const long long blocks = (long long)tiles_t * cgroups;
-    if (blocks > 0x7fffffffLL) return fail(KS_ERR_UNSUPPORTED, "ks_preprocess_int16: too many tiles");
-    const size_t smem = sizeof(float) * ((size_t)fir_taps_rounded(nt) + (size_t)kFirC * fir_window(nt));
     __nv_bfloat16* yhi = split ? reinterpret_cast<__nv_bfloat16*>(base + p.yhi) : nullptr;
     __nv_bfloat16* ylo = split ? reinterpret_cast<__nv_bfloat16*>(base + p.ylo) : nullptr;
-    if (split) {
-      KS_CUDA(cudaFuncSetAttribute(ks_pre_fir_kernel<true>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      ks_pre_fir_kernel<true><<<(unsigned)blocks, kFirThreads, smem, s>>>(
-          Xc, (int)C, (int)L, taps, nt, centre, tiles_t, check, artifact_threshold, nullptr, 0,
-          yhi, ylo,
-          (int)p.Cq, (int)p.Tpad, art);
+    if (hp_taps) {
+      int rc = ks::fir_tc(hp_taps, (int)ntaps, phi, plo, C, L, pcols, rows,
+                          reinterpret_cast<__nv_bfloat16*>(base + p.thi),
+                          reinterpret_cast<__nv_bfloat16*>(base + p.tlo), check,
+                          artifact_threshold, X, ldx, yhi, ylo, p.Cq, art, err, s);
+      if (rc) return rc;
     } else {
-      KS_CUDA(cudaFuncSetAttribute(ks_pre_fir_kernel<false>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      ks_pre_fir_kernel<false><<<(unsigned)blocks, kFirThreads, smem, s>>>(
-          Xc, (int)C, (int)L, taps, nt, centre, tiles_t, check, artifact_threshold, X, ldx,
-          nullptr, nullptr,
-          (int)p.Cq, 0, art);
+      // the split operand is written whole (Tpad rows, zeros past L)
+      const int nt = 1, centre = 0;
+      const int tiles_t = (int)((rows + kFirT - 1) / kFirT);
+      const int cgroups = (int)((split ? p.Cq : C) + kFirC - 1) / kFirC;
+      const long long blocks = (long long)tiles_t * cgroups;
+      if (blocks > 0x7fffffffLL) return fail(KS_ERR_UNSUPPORTED, "ks_preprocess_int16: too many tiles");
+      const size_t smem = sizeof(float) * ((size_t)fir_taps_rounded(nt) + (size_t)kFirC * fir_window(nt));
+      if (split) {
+        KS_CUDA(cudaFuncSetAttribute(ks_pre_fir_kernel<true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ks_pre_fir_kernel<true><<<(unsigned)blocks, kFirThreads, smem, s>>>(
+            Xc, (int)C, (int)L, nullptr, nt, centre, tiles_t, check, artifact_threshold, nullptr,
+            0, yhi, ylo, (int)p.Cq, (int)p.Tpad, art);
+      } else {
+        KS_CUDA(cudaFuncSetAttribute(ks_pre_fir_kernel<false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ks_pre_fir_kernel<false><<<(unsigned)blocks, kFirThreads, smem, s>>>(
+            Xc, (int)C, (int)L, nullptr, nt, centre, tiles_t, check, artifact_threshold, X, ldx,
+            nullptr, nullptr, (int)p.Cq, 0, art);
+      }
+      KS_CUDA(cudaGetLastError());
     }
-    KS_CUDA(cudaGetLastError());
     // 4. whitening on the tensor cores
     if (split) {
       __nv_bfloat16* whi = reinterpret_cast<__nv_bfloat16*>(base + p.whi);

@@ -70,6 +70,20 @@ int launch_project(const float* X, const float* U, const float* W, int64_t C,
                    int* err_out, cudaStream_t stream);
 int sgemm_tn(const float* A, const float* Bt, float* Cm, int64_t M, int64_t N,
              int64_t Kd, int64_t ldc, cudaStream_t stream, bool tiled);
+// High-pass FIR as a split-BF16 tcgen05 product with the Toeplitz matrix of
+// the taps (fir_tc.cu).  P hi/lo [C][cols] is the batch padded circularly
+// (P[c][j] = x[c][(j - h) mod L]) with cols = fir_tc_cols(rows, ntaps); the
+// output is rows x Cq bf16 hi/lo (yhi non-null; zeros past L and C) or f32
+// X[c][ldx]; |y| >= thr sets *art when check.  H hi/lo: scratch of
+// fir_tc_toeplitz_bytes(ntaps) / 2 bytes each.
+int64_t fir_tc_kpad(int ntaps);
+int64_t fir_tc_cols(int64_t rows, int ntaps);
+size_t fir_tc_toeplitz_bytes(int ntaps);
+int fir_tc(const float* taps, int ntaps, const __nv_bfloat16* p_hi, const __nv_bfloat16* p_lo,
+           int64_t C, int64_t L, int64_t cols, int64_t rows, __nv_bfloat16* h_hi,
+           __nv_bfloat16* h_lo, bool check, float thr, float* X, int64_t ldx,
+           __nv_bfloat16* yhi, __nv_bfloat16* ylo, int64_t Cq, int* art, int* err,
+           cudaStream_t stream);
 // Split-BF16 contraction on tcgen05: B = Uhi*Yhi^T + Uhi*Ylo^T + Ulo*Yhi^T.
 int gemm_bf16x3(const __nv_bfloat16* Uhi, const __nv_bfloat16* Ulo,
                 const __nv_bfloat16* Yhi, const __nv_bfloat16* Ylo, float* B,

@@ -27,6 +27,8 @@ falls back to ``bfile.padded_batch_to_torch`` when it does not.
 """
 from __future__ import annotations
 
+import threading
+import weakref
 from concurrent.futures import ThreadPoolExecutor
 from typing import Optional
 
@@ -153,9 +155,11 @@ class FilteredBatches:
 
     ``batch(ibatch, ops)`` enqueues the copy and the filter on the current
     stream and returns the batch tensor; ``check()`` synchronises with the
-    last filter and raises if the device reported an error.  The pinned
-    window buffer is reused: a call waits until the previous call's copy out
-    of it has finished.
+    last filter and raises if the device reported an error.  Two pinned
+    windows and two device copies of them alternate, so the host cuts the
+    next window while the previous one crosses to the device; a window is
+    rewritten only after its copy has finished, and its device copy only after
+    the filter that read it.
     """
 
     def __init__(self, bfile, device, copy_threads: int = 4, ntaps: int = 1023):
@@ -166,12 +170,13 @@ class FilteredBatches:
         self.device = torch.device(device)
         if self.device.type != "cuda":
             raise ValueError("FilteredBatches runs on a CUDA device")
+        self.signature = _signature(bfile)
         self.NT, self.nt = int(bfile.NT), int(bfile.nt)
         self.L = self.NT + 2 * self.nt
         self.n_chan_bin = int(bfile.n_chan_bin)
         whiten = bfile.whiten_mat
         if whiten is not None:
-            whiten = torch.as_tensor(whiten).detach().to(self.device, torch.float32)
+            whiten = torch.as_tensor(whiten).detach().to(self.device, torch.float32).clone()
         self.whiten = whiten
         self.pre = Preprocessor(self.n_chan_bin, self.L, whiten=whiten,
                                 chan_map=bfile.chan_map, hp_filter=bfile.hp_filter,
@@ -179,9 +184,13 @@ class FilteredBatches:
                                 artifact_threshold=float(bfile.artifact_threshold),
                                 device=self.device, ntaps=ntaps)
         self.C = self.pre.C
-        self.host = torch.empty((self.L, self.n_chan_bin), dtype=torch.int16).pin_memory()
-        self.raw = torch.empty((self.L, self.n_chan_bin), dtype=torch.int16, device=self.device)
-        self.copied = None                       # event: last copy out of self.host done
+        self.host = [torch.empty((self.L, self.n_chan_bin), dtype=torch.int16).pin_memory()
+                     for _ in range(2)]
+        self.raw = [torch.empty((self.L, self.n_chan_bin), dtype=torch.int16, device=self.device)
+                    for _ in range(2)]
+        self.copied = [None, None]               # events: copy out of host[i] done
+        self.used = [None, None]                 # events: filter of raw[i] done
+        self.slot = 0
         self.pool = ThreadPoolExecutor(copy_threads, thread_name_prefix="ks-window") \
             if copy_threads > 1 else None
 
@@ -204,16 +213,23 @@ class FilteredBatches:
         return drift_matrix(ops, dshift[int(ibatch)], self.device).to(torch.float32)
 
     def batch(self, ibatch: int, ops=None, out: Optional[torch.Tensor] = None) -> torch.Tensor:
-        if self.copied is not None:
-            self.copied.synchronize()
-        padded_window(self.bfile, ibatch, self.host.numpy(), copy=self._copy)
+        i = self.slot
+        self.slot ^= 1
+        if self.copied[i] is not None:
+            self.copied[i].synchronize()
+        padded_window(self.bfile, ibatch, self.host[i].numpy(), copy=self._copy)
         stream = torch.cuda.current_stream(self.device)
-        self.raw.copy_(self.host, non_blocking=True)
-        self.copied = torch.cuda.Event()
-        self.copied.record(stream)
+        if self.used[i] is not None:
+            stream.wait_event(self.used[i])
+        self.raw[i].copy_(self.host[i], non_blocking=True)
+        self.copied[i] = torch.cuda.Event()
+        self.copied[i].record(stream)
         if out is None:
             out = torch.empty((self.C, self.L), dtype=torch.float32, device=self.device)
-        return self.pre(self.raw, out, drift=self._drift(ops, ibatch))
+        X = self.pre(self.raw[i], out, drift=self._drift(ops, ibatch))
+        self.used[i] = torch.cuda.Event()
+        self.used[i].record(stream)
+        return X
 
     def check(self) -> None:
         status, _ = self.pre.status()
@@ -225,3 +241,45 @@ class FilteredBatches:
         if self.pool is not None:
             self.pool.shutdown(wait=True)
             self.pool = None
+
+
+def _tensor_key(t):
+    if t is None:
+        return None
+    if torch.is_tensor(t):
+        return ("tensor", id(t), t._version)
+    a = np.asarray(t)
+    return ("array", a.dtype.str, a.shape, a.tobytes())
+
+
+def _signature(bfile):
+    """What the device filter is built from: a file whose settings differ (a
+    new or changed channel map, filter or whitening tensor, other flags or
+    sizes) gets a new FilteredBatches."""
+    return (int(bfile.NT), int(bfile.nt), int(bfile.n_chan_bin), _dtype_name(bfile),
+            _tensor_key(bfile.chan_map), _tensor_key(bfile.hp_filter),
+            _tensor_key(bfile.whiten_mat), bool(bfile.do_CAR), bool(bfile.invert_sign),
+            float(bfile.artifact_threshold))
+
+
+_cache = weakref.WeakKeyDictionary()
+_cache_lock = threading.Lock()
+
+
+def batches_for(bfile, device) -> FilteredBatches:
+    """The FilteredBatches of ``bfile`` on ``device``, kept with the file object
+    (weakly) and reused while its settings are unchanged, so repeated
+    `extract` calls on one file keep their pinned windows and filter state."""
+    device = torch.device(device)
+    sig = _signature(bfile)
+    with _cache_lock:
+        try:
+            per_dev = _cache.setdefault(bfile, {})
+        except TypeError:                 # not weakly referenceable: no reuse
+            return FilteredBatches(bfile, device)
+        fb = per_dev.get(device)
+        if fb is None or fb.signature != sig:
+            if fb is not None:
+                fb.close()
+            fb = per_dev[device] = FilteredBatches(bfile, device)
+        return fb

@@ -414,6 +414,25 @@ def _match_features(ops, W, iCCd, iU, Ucc):
     return match, features
 
 
+_reader_pools = {}
+_reader_lock = threading.Lock()
+
+
+def _reader(device):
+    """(worker thread, stream) that read batches ahead for ``device``; kept for
+    the process, so repeated `extract` calls reuse the thread's library
+    handles."""
+    key = (device.type, device.index)
+    with _reader_lock:
+        r = _reader_pools.get(key)
+        if r is None:
+            from concurrent.futures import ThreadPoolExecutor
+            pool = ThreadPoolExecutor(1, thread_name_prefix="ks-batch-reader")
+            stream = torch.cuda.Stream(device) if device.type == "cuda" else None
+            r = _reader_pools[key] = (pool, stream)
+        return r
+
+
 class _BatchReader:
     """Reads padded batches one ahead on a worker thread, so the next batch's
     file read, host->device copy and filter overlap the current batch's
@@ -438,16 +457,15 @@ class _BatchReader:
         self.bfile, self.order, self.ops = bfile, list(order), ops
         self.device = torch.device(device) if device is not None else None
         self.pool = None
+        self.stream = None
         self.next = None
-        self.streams = {}
         self.filtered = None
         from . import filtered          # imports this module's stream helper
         if self.device is not None and self.device.type == "cuda" \
                 and ops.get("device_filter", True) and filtered.supports(bfile):
-            self.filtered = filtered.FilteredBatches(bfile, self.device)
+            self.filtered = filtered.batches_for(bfile, self.device)
         if ahead and len(self.order) > 1:
-            from concurrent.futures import ThreadPoolExecutor
-            self.pool = ThreadPoolExecutor(1, thread_name_prefix="ks-batch-reader")
+            self.pool, self.stream = _reader(self.device or torch.device("cpu"))
             self.next = self.pool.submit(self._read, self.order[0])
 
     def _load(self, ibatch):
@@ -461,9 +479,7 @@ class _BatchReader:
         dev = self.device
         if self.pool is None or dev is None or dev.type != "cuda":
             return self._load(ibatch)
-        if dev not in self.streams:
-            self.streams[dev] = torch.cuda.Stream(dev)
-        s = self.streams[dev]
+        s = self.stream
         with torch.cuda.device(dev), torch.cuda.stream(s):
             X = self._load(ibatch)
         s.synchronize()
@@ -481,18 +497,19 @@ class _BatchReader:
         return X
 
     def close(self):
-        if self.pool is not None:
-            if self.next is not None:
-                self.next.cancel()
-            self.pool.shutdown(wait=True)
-            self.pool = None
-        if self.filtered is not None:
-            self.filtered.close()
-            self.filtered = None
+        # leave no read of ours running on the shared worker
+        if self.next is not None and not self.next.cancel():
+            try:
+                self.next.result()
+            except Exception:
+                pass
+        self.next = None
+        self.pool = None
+        self.filtered = None
 
 
 def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=None,
-                    read_ahead=True):
+                    read_ahead=True, reader=None):
     """Rows ``[N, 3]`` (time, template, th_amp; float64 numpy) and features
     ``[N, nC, P]`` (CPU tensor) of the given batches, in batch order, before
     the final sort -- the loop body of kilosort/template_matching.py:79-110.
@@ -517,8 +534,9 @@ def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=N
     prog = tqdm(batches, miniters=200 if progress_bar else None,
                 mininterval=60 if progress_bar else None) if tqdm else batches
     ibatch = -1
-    reader = _BatchReader(bfile, [int(b) for b in batches], ops, device=U.device,
-                          ahead=read_ahead)
+    if reader is None:
+        reader = _BatchReader(bfile, [int(b) for b in batches], ops, device=U.device,
+                              ahead=read_ahead)
     try:
         for pos, ibatch in enumerate(prog):
             ibatch = int(ibatch)
@@ -571,18 +589,25 @@ def extract(ops, bfile, U, device=torch.device("cuda"), progress_bar=None):
     """
     nC = ops["settings"]["nearest_chans"]
     position_limit = ops["settings"]["position_limit"]
-    iCC, iCC_mask, iU, Ucc = prepare_extract(ops["xc"], ops["yc"], U, nC,
-                                             position_limit, device=device)
-    ops["iCC"] = iCC
-    ops["iCC_mask"] = iCC_mask
-    ops["iU"] = iU
-    ctc = prepare_matching(ops, U)
-    W = ops["wPCA"].contiguous()
-    iCCd = iCC.to(U.device).contiguous()
-    match, features = _match_features(ops, W, iCCd, iU, Ucc)
     batches = np.arange(bfile.n_batches, dtype=np.int64)
+    # the first batch is read (and filtered) while the templates are prepared
+    reader = _BatchReader(bfile, [int(b) for b in batches], ops, device=U.device,
+                          ahead=bool(ops.get("read_ahead", True)))
+    try:
+        iCC, iCC_mask, iU, Ucc = prepare_extract(ops["xc"], ops["yc"], U, nC,
+                                                 position_limit, device=device)
+        ops["iCC"] = iCC
+        ops["iCC_mask"] = iCC_mask
+        ops["iU"] = iU
+        ctc = prepare_matching(ops, U)
+        W = ops["wPCA"].contiguous()
+        iCCd = iCC.to(U.device).contiguous()
+        match, features = _match_features(ops, W, iCCd, iU, Ucc)
+    except Exception:
+        reader.close()
+        raise
     st, tF = extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar,
-                             read_ahead=bool(ops.get("read_ahead", True)))
+                             reader=reader)
     st, tF = sort_spikes(st, tF)
     return st, tF, ops
 
