@@ -17,6 +17,7 @@ of KS_BENCH_E2E_GROUP = 5 batches, copies and read-back beside the matching).
     python bench.py --workload uneven     # three recordings, 200 uneven batches
     python bench.py --workload adjoint    # reconstruction loss + adjoint
     python bench.py --workload extract    # drop-in extract over an int16 filtered file
+    python bench.py --workload filter     # the batch filter alone, one int16 batch
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -63,14 +64,15 @@ def parse():
     p.add_argument("--batches", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="np1",
-                   choices=["np1", "uneven", "adjoint", "stream", "detect", "extract"],
+                   choices=["np1", "uneven", "adjoint", "stream", "detect", "extract", "filter"],
                    help="np1: C=384/K=600, 20 equal batches (default); uneven: three "
                         "recordings, 200 batches of uneven length, batched launches; "
                         "adjoint: reconstruction loss + hand-written adjoint on one "
                         "C=384/K=600 batch with the matcher's spikes; stream: int16 host "
                         "stream -> whitening -> batched matcher, C=384/K=2000, with "
                         "periodic template refinement; extract: the drop-in extract over "
-                        "an int16 BinaryFiltered-style file, device batch filter")
+                        "an int16 BinaryFiltered-style file, device batch filter; filter: "
+                        "the batch filter alone on one 385-channel int16 batch")
     p.add_argument("--group", type=int, default=50,
                    help="uneven workload: batches per batched call (one graph each)")
     p.add_argument("--group-stream", type=int, default=4,
@@ -547,6 +549,57 @@ def stream_main(args, dev, rank, world):
         print(json.dumps(line), flush=True)
 
 
+FILTER = ("batch filter of one raw int16 batch on the device: 385 file channels (384 mapped), "
+          "60122 samples, mean, CAR median, 300 Hz high-pass (1023 taps, split-BF16 tcgen05 "
+          "Toeplitz product), whitening (split-BF16 tcgen05)")
+
+
+def filter_main(args, dev, rank, world):
+    """ks_preprocess_int16 on one resident raw batch (the kernel case of the
+    FIR profile)."""
+    from kilosort_b200 import synth
+    from kilosort_b200.preprocess import Preprocessor, highpass_filter
+    n_bin, L, C = 385, NT_BATCH + 2 * NT, 384
+    raw = synth.raw_batch(7101, n_bin, L, n_spikes=3000)
+    p = Preprocessor(n_bin, L, whiten=torch.eye(C) / 200.0, chan_map=np.arange(C),
+                     hp_filter=highpass_filter(), device=dev)
+    r = torch.from_numpy(raw).to(dev)
+    X = torch.empty((C, L), device=dev)
+    for _ in range(max(3, args.warmup)):
+        p(r, X)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev.index or 0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler.__enter__()
+    e0.record()
+    for _ in range(args.steps):
+        p(r, X)
+    e1.record()
+    torch.cuda.synchronize()
+    sampler.__exit__()
+    status = p.status()
+    if status[0] != 0:
+        raise RuntimeError(f"batch filter failed: {status}")
+    ms = e0.elapsed_time(e1) / args.steps
+    line = {
+        "metric": "channel-samples/s", "value": C * L * world / (ms * 1e-3),
+        "unit": "channel-samples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "int16 in, f32 out (split-bf16 FIR and whitening)", "data": "synthetic",
+        "config": {"workload": FILTER, "l2": "one 46 MB batch resident; the 92 MB padded "
+                   "operand and the 92 MB output exceed neither L2 nor its reuse",
+                   "parallelism": f"replicas x{world}"},
+        # FIR: 3 products x 2 flops x 128 x 192 x 1152 per tile, 940 tiles
+        "fir_gflop_per_step": 3 * 2 * 128 * 192 * 1152 * 940 / 1e9,
+        # sums, CAR, Toeplitz, FIR, matrix split, whitening, zeroing
+        "gpu_launches": 7 * args.steps,
+        "clocks": sampler.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 EXTRACT = ("drop-in extract over a BinaryFiltered-style int16 file in host memory: 385 file "
            "channels (384 mapped, NP1-like), K=600 templates, {nb} batches of 60000 samples, "
            "the reference's batch filter on the device (mean, CAR median, 300 Hz high-pass, "
@@ -572,7 +625,7 @@ def extract_main(args, dev, rank, world):
     Kxx = torch.from_numpy(np.exp(-d2 / (2 * 20.0 ** 2)))
     iKxx = torch.linalg.inv(Kxx + 0.01 * torch.eye(C)).to(dev)
     ops = dict(Th_learned=TH, nt=NT, max_peels=100, wPCA=torch.from_numpy(rec.wPCA).to(dev),
-               nt0min=20, batch_size=NT_BATCH, xc=xc, yc=yc, nblocks=1,
+               projection="bf16x3", nt0min=20, batch_size=NT_BATCH, xc=xc, yc=yc, nblocks=1,
                yblk=np.array([yc.mean()]), probe=dict(xc=xc, yc=yc), iKxx=iKxx,
                settings=dict(nearest_chans=10, position_limit=100, n_pcs=N_PCS, sig_interp=20.0))
     src = synth.FilteredBinary(raw, NT=NT_BATCH, nt=NT, chan_map=np.arange(C),
@@ -590,14 +643,22 @@ def extract_main(args, dev, rank, world):
         st, tF, _ = kb.extract(dict(ops), src, U, device=dev)
     dt = (time.perf_counter() - t0) / args.steps
     sampler.__exit__()
+    # the same extract with the plain-FP32 projection (the default of ops)
+    ops32 = dict(ops, projection="fp32")
+    kb.extract(dict(ops32), src, U, device=dev)
+    torch.cuda.synchronize()
+    t4 = time.perf_counter()
+    for _ in range(args.steps):
+        kb.extract(dict(ops32), src, U, device=dev)
+    dt32 = (time.perf_counter() - t4) / args.steps
     # the stages alone, one after the other: the batch source, then matching
-    fb = filtered.FilteredBatches(src, dev)
+    # (the file's device source, as extract left it: pinned windows in place)
+    fb = filtered.batches_for(src, dev)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     Xs = [fb.batch(b, ops) for b in range(nb)]
     fb.check()
     t_src = time.perf_counter() - t1
-    fb.close()
     ctc = kb.prepare_matching(ops, U)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
@@ -619,6 +680,7 @@ def extract_main(args, dev, rank, world):
                    "parallelism": f"replicas x{world}"},
         "spikes_per_step": len(st),
         "stages_ms": {"batch_source_alone": t_src * 1e3, "matching_alone": t_match * 1e3},
+        "fp32_projection": {"value": C * nb * NT_BATCH * world / dt32, "ms_per_step": dt32 * 1e3},
         # per batch: filter 6, matching 7, features 1; per call: template
         # channels, ctc (2), transpose
         "gpu_launches": 14 * nb + 4,
@@ -672,9 +734,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=dev)
 
-    if args.workload in ("uneven", "adjoint", "stream", "detect", "extract"):
+    if args.workload in ("uneven", "adjoint", "stream", "detect", "extract", "filter"):
         {"uneven": uneven_main, "adjoint": adjoint_main, "stream": stream_main,
-         "detect": detect_main, "extract": extract_main}[args.workload](args, dev, rank, world)
+         "detect": detect_main, "extract": extract_main,
+         "filter": filter_main}[args.workload](args, dev, rank, world)
         if world > 1:
             dist.destroy_process_group()
         return
