@@ -606,17 +606,18 @@ EXTRACT = ("drop-in extract over a BinaryFiltered-style int16 file in host memor
            "whitening with one-block drift correction), split-BF16 projection, PC features")
 
 
-def extract_main(args, dev, rank, world):
-    """kb.extract over a synth.FilteredBinary: host int16 file -> sorted host arrays."""
-    import kilosort_b200 as kb
-    from kilosort_b200 import filtered, synth
+def _extract_file(nb, reps, dev):
+    """The extract workload's file: nb batches of the NP1 recording (int16,
+    385 channels), repeated ``reps`` times along time for a sharded run, with
+    its ops (split projection, one-block drift) and templates."""
+    from kilosort_b200 import synth
     from kilosort_b200.preprocess import highpass_filter
-    nb = args.batches if args.batches != 20 else 8
     rec = synth.config_recording(CFG, n_batches=nb)
     C, n_bin = rec.n_chan, rec.n_chan + 1
     # raw = round(200 * whitened signal) + offsets, drifts, common mode and
     # noise of sd 20 on every file channel; whitening eye / 200 undoes the gain
     raw = synth.raw_recording(rec, n_bin, np.arange(C), seed=1102, gain=200.0)[:nb * NT_BATCH]
+    data = raw if reps == 1 else synth.TiledSamples(raw, reps)
     rng = np.random.default_rng(1103)
     W = torch.eye(C) / 200.0
     xc, yc = rec.xc.astype(np.float32), rec.yc.astype(np.float32)
@@ -628,10 +629,77 @@ def extract_main(args, dev, rank, world):
                projection="bf16x3", nt0min=20, batch_size=NT_BATCH, xc=xc, yc=yc, nblocks=1,
                yblk=np.array([yc.mean()]), probe=dict(xc=xc, yc=yc), iKxx=iKxx,
                settings=dict(nearest_chans=10, position_limit=100, n_pcs=N_PCS, sig_interp=20.0))
-    src = synth.FilteredBinary(raw, NT=NT_BATCH, nt=NT, chan_map=np.arange(C),
+    src = synth.FilteredBinary(data, NT=NT_BATCH, nt=NT, chan_map=np.arange(C),
                                hp_filter=highpass_filter(), whiten_mat=W,
-                               dshift=rng.uniform(-5.0, 5.0, (nb, 1)), device=dev)
-    assert src.n_batches == nb and filtered.supports(src)
+                               dshift=rng.uniform(-5.0, 5.0, (nb * reps, 1)), device=dev)
+    assert src.n_batches == nb * reps
+    return rec, raw, src, ops, torch.from_numpy(rec.U).to(dev)
+
+
+def extract_sharded_block(args, dev, rank, world, nb=8):
+    """sharding.extract_sharded over nb batches per rank (weak scaling): the
+    file repeats the nb-batch recording once per rank, rank r matches batches
+    [r nb, (r+1) nb), rows and features gather on rank 0, which sorts them.
+    Host wall clock per rank between barriers, max over ranks."""
+    import torch.distributed as dist
+    from kilosort_b200 import sharding
+    _, _, src, ops, U = _extract_file(nb, world, dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(1, args.warmup)):
+        sharding.extract_sharded(dict(ops), src, U, device=dev)
+    barrier()
+    t0 = time.perf_counter()
+    n = 0
+    for _ in range(args.steps):
+        st, _, _ = sharding.extract_sharded(dict(ops), src, U, device=dev)
+        n = len(st) if st is not None else n
+    torch.cuda.synchronize()
+    dt = torch.tensor([(time.perf_counter() - t0) / args.steps], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(dt, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    dt = float(dt.item())
+    C = len(src.chan_map)
+    return {"value": C * nb * world * NT_BATCH / dt, "unit": "channel-samples/s",
+            "ms_per_step": dt * 1e3, "batches_per_rank": nb, "spikes_per_step": n,
+            "scaling": "weak",
+            "timing": "host wall clock per rank (int16 file in, sorted st/tF on rank 0 out), "
+                      "max over ranks"}
+
+
+def extract_main(args, dev, rank, world):
+    """kb.extract over a synth.FilteredBinary: host int16 file -> sorted host
+    arrays; with several ranks, sharding.extract_sharded over nb batches per
+    rank."""
+    import kilosort_b200 as kb
+    from kilosort_b200 import filtered, synth
+    nb = args.batches if args.batches != 20 else 8
+    if world > 1:
+        blk = extract_sharded_block(args, dev, rank, world, nb)
+        line = {"metric": "channel-samples/s", "value": blk["value"],
+                "unit": "channel-samples/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": blk["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "int16 in, f32 (f32 filter, split-bf16 whitening and projection)",
+                "data": "synthetic",
+                "config": {"workload": EXTRACT.format(nb=nb) + ", per rank",
+                           "parallelism": f"batch shards x{world} (sharding.extract_sharded)"},
+                "extract_sharded": blk,
+                "e2e": {"value": blk["value"], "unit": "channel-samples/s",
+                        "h2d_bytes_per_step": nb * (NT_BATCH + 2 * NT) * 385 * 2 * world,
+                        "d2h_bytes_per_step": None}}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
+    rec, raw, src, ops, U = _extract_file(nb, 1, dev)
+    C, n_bin = rec.n_chan, rec.n_chan + 1
+    W = src.whiten_mat
+    assert filtered.supports(src)
     U = torch.from_numpy(rec.U).to(dev)
     for _ in range(max(1, args.warmup)):
         kb.extract(dict(ops), src, U, device=dev)
@@ -1046,6 +1114,9 @@ def main():
         # batch, grouped contraction, peel, residual
         "gpu_launches": (3 + nb + 3) if head == "bf16x3_batched" else launches_per_batch * nb,
     }
+    # the drop-in extract sharded over the ranks (every rank takes part)
+    del Xs, Xh
+    line["extract_sharded"] = extract_sharded_block(args, dev, rank, world)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -439,3 +439,37 @@ class FilteredBinary:
         X = self._device_batches.batch(ibatch, ops)
         self._device_batches.check()
         return X
+
+
+class TiledSamples:
+    """A read-only ``[reps * T, n_chan_bin]`` sample array that repeats ``base``
+    ``reps`` times along time, without copying it: a long file for the
+    sharded benchmark (every rank's batches hold the same recording).
+    Slicing returns a numpy array (a copy where the slice crosses a repeat)."""
+
+    def __init__(self, base: np.ndarray, reps: int):
+        self.base = base
+        self.reps = int(reps)
+        self.dtype = base.dtype
+        self.shape = (base.shape[0] * self.reps, base.shape[1])
+
+    def __len__(self):
+        return self.shape[0]
+
+    def __getitem__(self, idx):
+        if not isinstance(idx, slice) or idx.step not in (None, 1):
+            raise TypeError("TiledSamples supports contiguous time slices only")
+        start, stop, _ = idx.indices(self.shape[0])
+        T = self.base.shape[0]
+        if stop <= start:
+            return self.base[:0]
+        if start // T == (stop - 1) // T:
+            o = (start // T) * T
+            return self.base[start - o:stop - o]
+        parts, s = [], start
+        while s < stop:
+            o = (s // T) * T
+            e = min(stop, o + T)
+            parts.append(self.base[s - o:e - o])
+            s = e
+        return np.concatenate(parts, 0)

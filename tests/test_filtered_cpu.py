@@ -153,3 +153,14 @@ def test_oracle_padded_batch_equals_reference_windows(case):
         assert _sha(X.numpy().astype(np.int16)) == str(G["window_sha"][b]), b
     u = _source((raw.astype(np.int32) + 32768).astype(np.uint16))
     assert torch.equal(op.padded_batch(u, 2, "cpu"), op.padded_batch(src, 2, "cpu"))
+
+
+def test_tiled_samples_repeat_the_base_file():
+    base = np.arange(60, dtype=np.int16).reshape(20, 3)
+    t = synth.TiledSamples(base, 4)
+    full = np.concatenate([base] * 4)
+    assert t.shape == full.shape and t.dtype == base.dtype
+    for s, e in [(0, 20), (3, 17), (18, 23), (5, 75), (0, 80), (79, 80), (40, 40)]:
+        np.testing.assert_array_equal(t[s:e], full[s:e])
+    src = synth.FilteredBinary(t, NT=9, nt=2, device="cpu")
+    assert src.n_batches == int(np.ceil(80 / 9))
