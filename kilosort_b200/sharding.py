@@ -101,6 +101,26 @@ def extract_sharded(ops, bfile, U, device=None, dst: int = 0, group=None,
     world = dist.get_world_size(group) if distributed else 1
     if distributed:
         broadcast_templates(U, ops["wPCA"], src=dst, group=group)
+    start, stop = batch_range(int(bfile.n_batches), world, rank)
+    batches = np.arange(start, stop, dtype=np.int64)
+    # this rank's first batch is read while the templates are prepared
+    reader = tm._BatchReader(bfile, [int(b) for b in batches], ops, device=U.device,
+                             ahead=bool(ops.get("read_ahead", True)))
+    try:
+        st, tF = _match_range(ops, bfile, batches, U, device, match, features, prepare,
+                              progress_bar, reader)
+    finally:
+        reader.close()
+    if distributed:
+        st, tF = _gather_rows(st, tF, dst, group)
+        if rank != dst:
+            return None, None, ops
+    st, tF = tm.sort_spikes(st, tF)
+    return st, tF, ops
+
+
+def _match_range(ops, bfile, batches, U, device, match, features, prepare, progress_bar,
+                 reader):
     if prepare is None:
         def prepare(o, Ut):
             iCC, iCC_mask, iU, Ucc = tm.prepare_extract(
@@ -114,16 +134,8 @@ def extract_sharded(ops, bfile, U, device=None, dst: int = 0, group=None,
         m, f = tm._match_features(ops, W, iCC.to(U.device).contiguous(), iU, Ucc)
         match = match or m
         features = features or f
-    start, stop = batch_range(int(bfile.n_batches), world, rank)
-    st, tF = tm.extract_batches(ops, bfile, np.arange(start, stop, dtype=np.int64), U, ctc,
-                                match, features, progress_bar,
-                                read_ahead=bool(ops.get("read_ahead", True)))
-    if distributed:
-        st, tF = _gather_rows(st, tF, dst, group)
-        if rank != dst:
-            return None, None, ops
-    st, tF = tm.sort_spikes(st, tF)
-    return st, tF, ops
+    return tm.extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar,
+                              reader=reader)
 
 
 def allreduce_gradients(tensors: Sequence[torch.Tensor], group=None):
