@@ -18,9 +18,11 @@
 // Kernels (C = selected channels, L = batch samples):
 //   ks_pre_sum_kernel   per-channel sums in double (int16 values: exact)
 //   ks_pre_car_kernel   32-sample tiles: centred values into shared memory,
-//                       per-sample lower median by a warp radix select on the
-//                       order-preserving integer keys of the floats, coalesced
-//                       [C][L] rows out
+//                       per-sample lower median by one warp: counts in 256
+//                       buckets over mean -/+ 4 sd, then an exact rank among the
+//                       few values of the median's bucket (a radix select on the
+//                       order-preserving integer keys when that bucket is
+//                       crowded); coalesced [C][L] rows out
 //                       (with a high-pass: the bf16 hi/lo samples of the
 //                       circularly padded batch P[c][j] = x[c][(j - h) mod L]
 //                       instead, the operand of the tensor-core FIR)
@@ -127,6 +129,107 @@ __device__ float warp_select(const float* tile, int pitch, int C, int s, int k, 
   return key_value(prefix);
 }
 
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Bucket of v among 256 over [lo, lo + 256 / inv): a non-decreasing function of
+// v (a rounded difference, a rounded product by inv > 0, truncation, clamping).
+__device__ __forceinline__ int median_bucket(float v, float lo, float inv) {
+  const float t = __fmul_rn(__fsub_rn(v, lo), inv);
+  return t < 0.f ? 0 : (t >= 255.f ? 255 : (int)t);
+}
+
+// Rank-k value (0-based, ascending) of column s of the tile, by one warp.
+// The values are counted into 256 buckets over mean -/+ 4 sd of the column
+// (outliers clamp to the end buckets); the bucket that holds rank k is found
+// from the counts, and since the bucket is a non-decreasing function of the
+// value, the rank-k value is the (k - values below the bucket)-th smallest of
+// that bucket's values, ranked exactly by comparisons.  Near the median the
+// buckets hold a few values each, so the shared-memory counts hardly collide.
+// A bucket of more than 32 values, or a zero or non-finite spread, goes to the
+// radix select.
+__device__ float warp_median(const float* tile, int pitch, int C, int s, int k, int* hist,
+                             float* cand, int* ncand) {
+  const int lane = threadIdx.x & 31;
+  float sum = 0.f, sq = 0.f;
+  for (int c = lane; c < C; c += 32) {
+    const float v = tile[c * pitch + s];
+    sum += v;
+    sq = fmaf(v, v, sq);
+  }
+  sum = warp_sum(sum);
+  sq = warp_sum(sq);
+  const float mean = sum / (float)C;
+  const float sd = sqrtf(fmaxf(sq / (float)C - mean * mean, 0.f));
+  const float lo = mean - 4.f * sd;
+  const float inv = 32.f / sd;                 // 256 buckets over 8 sd
+  if (!(sd > 0.f) || !isfinite(inv) || !isfinite(lo))
+    return warp_select(tile, pitch, C, s, k, hist);
+#pragma unroll
+  for (int b = 0; b < 8; ++b) hist[lane * 8 + b] = 0;
+  if (lane == 0) *ncand = 0;
+  __syncwarp();
+  for (int c = lane; c < C; c += 32)
+    atomicAdd(hist + median_bucket(tile[c * pitch + s], lo, inv), 1);
+  __syncwarp();
+  int cnt[8], local = 0;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    cnt[b] = hist[lane * 8 + b];
+    local += cnt[b];
+  }
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int excl = incl - local;
+  const unsigned hit = __ballot_sync(0xffffffffu, excl <= k && k < incl);
+  const int src = __ffs(hit) - 1;
+  int sel = 0, before = 0, m = 0;
+  if (lane == src) {
+    int acc = excl;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      if (k < acc + cnt[b]) {
+        sel = lane * 8 + b;
+        before = acc;
+        m = cnt[b];
+        break;
+      }
+      acc += cnt[b];
+    }
+  }
+  sel = __shfl_sync(0xffffffffu, sel, src);
+  before = __shfl_sync(0xffffffffu, before, src);
+  m = __shfl_sync(0xffffffffu, m, src);
+  if (m > 32) {
+    __syncwarp();
+    return warp_select(tile, pitch, C, s, k, hist);
+  }
+  for (int c = lane; c < C; c += 32) {
+    const float v = tile[c * pitch + s];
+    if (median_bucket(v, lo, inv) == sel) cand[atomicAdd(ncand, 1)] = v;
+  }
+  __syncwarp();
+  const int kk = k - before;
+  const float mine = lane < m ? cand[lane] : 0.f;
+  int less = 0, leq = 0;
+  for (int j = 0; j < m; ++j) {
+    const float o = cand[j];
+    less += o < mine ? 1 : 0;
+    leq += o <= mine ? 1 : 0;
+  }
+  const unsigned win = __ballot_sync(0xffffffffu, lane < m && less <= kk && kk < leq);
+  const float r = cand[__ffs(win) - 1];
+  __syncwarp();
+  return r;
+}
+
 // Centred (and common-average-referenced) samples: Xc[c][t], t < L; with kPad
 // instead the bf16 hi/lo planes of the circularly padded batch
 // P[c][j] = x[c][(j - h) mod L], j < cols (sample t at every j = t + h mod L).
@@ -142,6 +245,8 @@ ks_pre_car_kernel(const int16_t* __restrict__ raw, int L, long long ldr,
   float* tile = sm;                                        // [C][pitch]
   int* hist = reinterpret_cast<int*>(tile + (size_t)C * pitch);   // [8 warps][256]
   float* med = reinterpret_cast<float*>(hist + 8 * 256);   // [kCarTile]
+  float* cand = med + kCarTile;                            // [8 warps][32]
+  int* ncand = reinterpret_cast<int*>(cand + 8 * 32);      // [8 warps]
   const int t0 = blockIdx.x * kCarTile;
   const int nt = min(kCarTile, L - t0);
   for (int e = threadIdx.x; e < nt * C; e += kCarThreads) {
@@ -149,7 +254,9 @@ ks_pre_car_kernel(const int16_t* __restrict__ raw, int L, long long ldr,
     const long long m = map ? map[c] : c;
     float v = 0.f;
     if (m >= 0 && m < ldr) {
-      const float mean = (float)(sums[c] / (double)L);
+      // the mean of the (sign-inverted) samples: negation commutes with the
+      // rounded mean and difference, so this is fl(sign * raw - mean(sign * raw))
+      const float mean = sign * (float)(sums[c] / (double)L);
       v = __fsub_rn(sign * (float)raw[(long long)(t0 + s) * ldr + m], mean);
     } else {
       atomicCAS(err, 0, KS_ERR_ARG);
@@ -160,7 +267,8 @@ ks_pre_car_kernel(const int16_t* __restrict__ raw, int L, long long ldr,
   if (kCar) {
     const int warp = threadIdx.x >> 5;
     for (int s = warp; s < nt; s += kCarThreads / 32) {
-      const float m = warp_select(tile, pitch, C, s, (C - 1) / 2, hist + warp * 256);
+      const float m = warp_median(tile, pitch, C, s, (C - 1) / 2, hist + warp * 256,
+                                  cand + warp * 32, ncand + warp);
       if ((threadIdx.x & 31) == 0) med[s] = m;
     }
     __syncthreads();
@@ -384,7 +492,7 @@ extern "C" KS_API int ks_preprocess_int16(const int16_t* raw, int64_t L, int64_t
   __nv_bfloat16* plo = reinterpret_cast<__nv_bfloat16*>(base + p.plo);
   {
     const size_t smem = sizeof(float) * (size_t)C * (kCarTile + 1) + sizeof(int) * 8 * 256 +
-                        sizeof(float) * kCarTile;
+                        sizeof(float) * kCarTile + sizeof(float) * 8 * 32 + sizeof(int) * 8;
     const unsigned grid = (unsigned)((L + kCarTile - 1) / kCarTile);
     const float sign = invert_sign ? -1.f : 1.f;
     auto run = [&](auto kernel) -> int {

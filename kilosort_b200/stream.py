@@ -196,6 +196,12 @@ class StreamMatcher:
         self.done[g % 2].record(cur)
 
     def _refine(self, m: BatchedMatcher):
+        """One gradient step on U from the reconstruction loss of the group's
+        first batch, on each template's footprint only: the channels whose
+        loading norm is at least 1e-3 of the template's largest.  Templates
+        stay as sparse as they were (Kilosort4's live on their nearest
+        channels); a dense step would spread every template over the probe
+        and, through ctc, make every peel update touch every template group."""
         st, amps, _, _ = m.results()[0]
         if len(st) == 0:
             return
@@ -203,7 +209,9 @@ class StreamMatcher:
         loss = reconstruction_loss(m.X[0], st, amps.reshape(-1), Uq, self.ops["wPCA"])
         loss.backward()
         with torch.no_grad():
-            self.U.sub_(self.refine_lr * Uq.grad)
+            norm = self.U.norm(dim=1)                                   # [K, C]
+            support = norm >= 1e-3 * norm.amax(dim=1, keepdim=True)
+            self.U.sub_(self.refine_lr * Uq.grad * support.unsqueeze(1))
             self.ctc.copy_(prepare_matching(self.ops, self.U))
             lib = _lib.load()
             K = self.U.shape[0]

@@ -40,6 +40,8 @@ CASES = {
     "drift": (704, 1100, False, True, True, np.inf, True, 7.5),
     "nohp": (705, 1100, False, True, False, np.inf, False, None),
     "odd": (706, 1101, False, True, True, 1e9, True, None),
+    "car_invert": (707, 1100, True, True, True, np.inf, True, None),
+    "car_invert_nohp": (708, 1100, True, True, False, np.inf, False, None),
 }
 
 

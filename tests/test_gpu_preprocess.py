@@ -129,3 +129,48 @@ def test_single_channel_and_odd_length(cuda_device):
     ref = op.filter_batch(torch.from_numpy(raw.T.astype(np.float64)), chan_map=torch.tensor([2]),
                           do_car=False, hp=hp.double()).numpy()
     assert np.abs(X - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+def _car_expected(raw, cmap, invert, car):
+    """The centring and common average reference in float32, as the kernel
+    rounds them: the per-channel mean of the integer samples (exact sum in
+    int64, divided in float64, rounded to float32, sign applied), one rounded
+    difference, then the lower median of each sample over channels and one
+    more rounded difference (torch.median of an even count is the lower one)."""
+    x = raw[:, cmap].astype(np.float32)
+    L, C = x.shape
+    sign = np.float32(-1.0 if invert else 1.0)
+    mean = (raw[:, cmap].astype(np.int64).sum(0).astype(np.float64) / L).astype(np.float32)
+    v = sign * x - sign * mean
+    if car:
+        med = np.sort(v, axis=1)[:, (C - 1) // 2]
+        v = v - med[:, None]
+    return v.T
+
+
+@pytest.mark.parametrize("C,L,kind,invert", [
+    (384, 1100, "noise", False), (384, 1100, "noise", True), (63, 1037, "ties", False),
+    (1000, 515, "noise", True), (2, 300, "noise", False), (1, 300, "noise", False),
+    (384, 700, "crowded", False), (384, 700, "outliers", True)])
+def test_car_median_exact(cuda_device, C, L, kind, invert):
+    """The CAR output equals the float32 host computation bit for bit: bucketed
+    median (noise, ties, outliers) and its radix-select fallback (a crowded
+    median bucket: 300 of 384 channels equal)."""
+    rng = np.random.default_rng(C * 1000 + L)
+    n_bin = C + 3
+    cmap = rng.permutation(n_bin)[:C]
+    if kind == "ties":
+        raw = rng.integers(-3, 4, (L, n_bin))
+    else:
+        raw = rng.normal(0, 40, (L, n_bin)) + rng.uniform(-300, 300, n_bin)
+    if kind == "crowded":
+        raw[:, cmap[:300]] = 17
+    if kind == "outliers":
+        hit = rng.random((L, n_bin)) < 0.05
+        raw[hit] = rng.choice([-30000, 30000], hit.sum())
+    raw = np.clip(np.round(raw), -32768, 32767).astype(np.int16)
+    for car in (True, False):
+        p = Preprocessor(n_bin, L, chan_map=cmap, do_CAR=car, invert_sign=invert, device=DEV)
+        X = p(torch.from_numpy(raw).to(DEV)).cpu().numpy()
+        assert p.status() == (_lib.KS_OK, False)
+        np.testing.assert_array_equal(X, _car_expected(raw, cmap, invert, car))

@@ -95,6 +95,10 @@ def test_stream_refinement_updates_templates(cuda_device):
     sm.close()
     assert sm.refinements >= 2
     assert not torch.equal(U, U0)
+    # only each template's footprint moves (channels within 1e-3 of its peak norm)
+    norm = U0.norm(dim=1)
+    off = (norm < 1e-3 * norm.amax(dim=1, keepdim=True)).unsqueeze(1).expand_as(U)
+    assert off.any() and torch.equal(U[off], U0[off])
     assert len(times) > 100
     # ctc follows the refined templates
     ctc_now = kb.prepare_matching(ops, U)
