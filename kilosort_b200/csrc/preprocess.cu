@@ -249,19 +249,19 @@ ks_pre_car_kernel(const int16_t* __restrict__ raw, int L, long long ldr,
   int* ncand = reinterpret_cast<int*>(cand + 8 * 32);      // [8 warps]
   const int t0 = blockIdx.x * kCarTile;
   const int nt = min(kCarTile, L - t0);
-  for (int e = threadIdx.x; e < nt * C; e += kCarThreads) {
-    const int s = e / C, c = e - s * C;
+  for (int c = threadIdx.x; c < C; c += kCarThreads) {
     const long long m = map ? map[c] : c;
-    float v = 0.f;
-    if (m >= 0 && m < ldr) {
-      // the mean of the (sign-inverted) samples: negation commutes with the
-      // rounded mean and difference, so this is fl(sign * raw - mean(sign * raw))
-      const float mean = sign * (float)(sums[c] / (double)L);
-      v = __fsub_rn(sign * (float)raw[(long long)(t0 + s) * ldr + m], mean);
-    } else {
+    if (m < 0 || m >= ldr) {
       atomicCAS(err, 0, KS_ERR_ARG);
+      for (int s = 0; s < nt; ++s) tile[c * pitch + s] = 0.f;
+      continue;
     }
-    tile[c * pitch + s] = v;
+    // the mean of the (sign-inverted) samples: negation commutes with the
+    // rounded mean and difference, so this is fl(sign * raw - mean(sign * raw))
+    const float mean = sign * (float)(sums[c] / (double)L);
+    const int16_t* src = raw + (long long)t0 * ldr + m;
+    for (int s = 0; s < nt; ++s)
+      tile[c * pitch + s] = __fsub_rn(sign * (float)src[(long long)s * ldr], mean);
   }
   __syncthreads();
   if (kCar) {
@@ -281,7 +281,10 @@ ks_pre_car_kernel(const int16_t* __restrict__ raw, int L, long long ldr,
       if (kPad) {
         const __nv_bfloat16 hv = __float2bfloat16_rn(y);
         const __nv_bfloat16 lv = __float2bfloat16_rn(y - __bfloat162float(hv));
-        for (long long j = (t0 + s + h) % L; j < cols; j += L) {
+        // t0 + s < L and h < L: the first position is one subtraction away
+        long long j = t0 + s + h;
+        if (j >= L) j -= L;
+        for (; j < cols; j += L) {
           Phi[(size_t)c * cols + j] = hv;
           Plo[(size_t)c * cols + j] = lv;
         }
