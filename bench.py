@@ -722,10 +722,11 @@ def extract_main(args, dev, rank, world):
     # the stages alone, one after the other: the batch source, then matching
     # (the file's device source, as extract left it: pinned windows in place)
     fb = filtered.batches_for(src, dev)
-    torch.cuda.synchronize()
+    fb.batch(0, ops)                      # this thread's first use (library handles)
+    fb.check()
     t1 = time.perf_counter()
     Xs = [fb.batch(b, ops) for b in range(nb)]
-    fb.check()
+    fb.check()                            # synchronises with the last filter
     t_src = time.perf_counter() - t1
     ctc = kb.prepare_matching(ops, U)
     torch.cuda.synchronize()

@@ -139,6 +139,19 @@ KS_API int ks_features(const float* Xres, const int64_t* st, const float* amps,
                 void* stream);
 
 /*
+ * ks_features for the first min(max_spikes, *n_spikes_dev) spikes, the count
+ * read on the device (an int64 a peel wrote, e.g. word 0 of its info), so the
+ * features can be enqueued behind the peel without reading the count back.
+ * tF holds max_spikes rows; rows past the count are left as they are.
+ * Replaces kilosort/template_matching.py:85-86 like ks_features.
+ */
+KS_API int ks_features_counted(const float* Xres, const int64_t* st, const float* amps,
+                               const float* W, const int64_t* iCC, const int64_t* iU,
+                               const float* Ucc, int64_t C, int64_t L, int64_t K, int64_t P,
+                               int64_t nt, int64_t nC, const int64_t* n_spikes_dev,
+                               int64_t max_spikes, float* tF, void* stream);
+
+/*
  * Per-template peak channel and feature loadings: iU[k] = argmax_c
  * sum_p U[k,p,c]^2 (first index on ties), Ucc[i,k,p] = U[k,p,iCC[i,iU[k]]].
  * Replaces the device part of kilosort/template_matching.py:50-51.

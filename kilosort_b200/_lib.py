@@ -54,6 +54,8 @@ SIGNATURES = {
     "ks_ctc_transpose": (_int, [_vp, _i64, _i64, _vp, _vp]),
     "ks_features": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64,
                            _i64, _i64, _i64, _i64, _vp, _vp]),
+    "ks_features_counted": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64,
+                                   _i64, _i64, _i64, _vp, _i64, _vp, _vp]),
     "ks_template_channels": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp]),
     "ks_ctc_workspace_size": (_sz, [_i64, _i64, _i64, _i64]),
     "ks_ctc": (_int, [_vp, _vp, _i64, _i64, _i64, _i64, _vp, _vp, _sz, _vp]),

@@ -71,7 +71,7 @@ int launch_ctc(const float* U, const float* W, int64_t K, int64_t P, int64_t C,
 int launch_features(const float* Xres, const int64_t* st, const float* amps,
                     const float* W, const int64_t* iCC, const int64_t* iU,
                     const float* Ucc, int64_t C, int64_t L, int64_t K, int64_t P,
-                    int64_t nt, int64_t nC, int64_t N, float* tF, cudaStream_t stream);
+                    int64_t nt, int64_t nC, int64_t N, float* tF, cudaStream_t stream, const int64_t* n_dev = nullptr);
 int launch_template_channels(const float* U, const int64_t* iCC, int64_t K,
                              int64_t P, int64_t C, int64_t nC, int64_t* iU,
                              float* Ucc, cudaStream_t stream);
@@ -286,6 +286,16 @@ int ks_features(const float* Xres, const int64_t* st, const float* amps,
                 int64_t nt, int64_t nC, int64_t n_spikes, float* tF, void* stream) {
   return launch_features(Xres, st, amps, W, iCC, iU, Ucc, C, L, K, P, nt, nC, n_spikes,
                          tF, static_cast<cudaStream_t>(stream));
+}
+
+int ks_features_counted(const float* Xres, const int64_t* st, const float* amps,
+                        const float* W, const int64_t* iCC, const int64_t* iU,
+                        const float* Ucc, int64_t C, int64_t L, int64_t K, int64_t P,
+                        int64_t nt, int64_t nC, const int64_t* n_spikes_dev,
+                        int64_t max_spikes, float* tF, void* stream) {
+  if (!n_spikes_dev) return fail(KS_ERR_ARG, "ks_features_counted: null count");
+  return launch_features(Xres, st, amps, W, iCC, iU, Ucc, C, L, K, P, nt, nC, max_spikes,
+                         tF, static_cast<cudaStream_t>(stream), n_spikes_dev);
 }
 
 int ks_template_channels(const float* U, const int64_t* iCC, int64_t K, int64_t P,

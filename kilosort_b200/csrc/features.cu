@@ -19,13 +19,17 @@ ks_features_kernel(const float* __restrict__ Xres, const long long* __restrict__
                    const float* __restrict__ amps, const float* __restrict__ W,
                    const long long* __restrict__ iCC, const long long* __restrict__ iU,
                    const float* __restrict__ Ucc, int C, int L, int K, int P,
-                   int nt, int nC, long long N, float* __restrict__ tF) {
+                   int nt, int nC, long long N, const long long* __restrict__ n_dev,
+                   float* __restrict__ tF) {
+  // with n_dev, the spikes to process are min(N, *n_dev) (a count the peel wrote)
+  const long long n = n_dev ? min(N, max(*n_dev, 0LL)) : N;
+  if ((long long)blockIdx.x * kFeatWarps >= n) return;
   extern __shared__ float sW[];  // [P][nt]
   for (int i = threadIdx.x; i < P * nt; i += blockDim.x) sW[i] = W[i];
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const long long s = (long long)blockIdx.x * kFeatWarps + (threadIdx.x >> 5);
-  if (s >= N) return;
+  if (s >= n) return;
   const long long tau = st[2 * s];
   const long long kk = st[2 * s + 1];
   const long long t0 = tau - nt / 2;
@@ -105,7 +109,7 @@ int launch_features(const float* Xres, const int64_t* st, const float* amps,
                     const float* W, const int64_t* iCC, const int64_t* iU,
                     const float* Ucc, int64_t C, int64_t L, int64_t K, int64_t P,
                     int64_t nt, int64_t nC, int64_t N, float* tF,
-                    cudaStream_t stream) {
+                    cudaStream_t stream, const int64_t* n_dev) {
   if (N == 0) return KS_OK;
   if (!Xres || !st || !amps || !W || !iCC || !iU || !Ucc || !tF)
     return fail(KS_ERR_ARG, "ks_features: null pointer");
@@ -116,7 +120,8 @@ int launch_features(const float* Xres, const int64_t* st, const float* amps,
   ks_features_kernel<<<(unsigned)blocks, kFeatWarps * 32, smem, stream>>>(
       Xres, reinterpret_cast<const long long*>(st), amps, W,
       reinterpret_cast<const long long*>(iCC), reinterpret_cast<const long long*>(iU), Ucc,
-      (int)C, (int)L, (int)K, (int)P, (int)nt, (int)nC, N, tF);
+      (int)C, (int)L, (int)K, (int)P, (int)nt, (int)nC, N,
+      reinterpret_cast<const long long*>(n_dev), tF);
   KS_CUDA(cudaGetLastError());
   return KS_OK;
 }

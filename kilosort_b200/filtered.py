@@ -37,6 +37,7 @@ import torch
 
 from . import _lib
 from .preprocess import Preprocessor
+from .template_matching import to_host
 
 # attributes of the reference's BinaryFiltered (io.py:569-659, 968-988) that
 # the device path reads
@@ -191,6 +192,8 @@ class FilteredBatches:
         self.copied = [None, None]               # events: copy out of host[i] done
         self.used = [None, None]                 # events: filter of raw[i] done
         self.slot = 0
+        # the largest device status of every batch filtered since the last check
+        self.sticky = torch.zeros(1, dtype=torch.int32, device=self.device)
         self.pool = ThreadPoolExecutor(copy_threads, thread_name_prefix="ks-window") \
             if copy_threads > 1 else None
 
@@ -227,12 +230,16 @@ class FilteredBatches:
         if out is None:
             out = torch.empty((self.C, self.L), dtype=torch.float32, device=self.device)
         X = self.pre(self.raw[i], out, drift=self._drift(ops, ibatch))
+        torch.maximum(self.sticky, self.pre.flags[:1], out=self.sticky)
         self.used[i] = torch.cuda.Event()
         self.used[i].record(stream)
         return X
 
     def check(self) -> None:
-        status, _ = self.pre.status()
+        """Raise if any batch filtered since the last check reported an error
+        (synchronises with the last one)."""
+        status = int(to_host(self.sticky)[0][0])
+        self.sticky.zero_()
         if status != _lib.KS_OK:
             raise _lib.KilosortB200Error(
                 status, f"ks_preprocess_int16: device status {_lib.status_message(status)}")

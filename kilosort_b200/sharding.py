@@ -103,12 +103,17 @@ def extract_sharded(ops, bfile, U, device=None, dst: int = 0, group=None,
         broadcast_templates(U, ops["wPCA"], src=dst, group=group)
     start, stop = batch_range(int(bfile.n_batches), world, rank)
     batches = np.arange(start, stop, dtype=np.int64)
-    # this rank's first batch is read while the templates are prepared
+    bgroup = int(ops.get("batch_group", 4))
+    ahead = bool(ops.get("read_ahead", True))
+    # this library's matcher: groups of batches per launch, as `extract` does
+    grouped = (match is None and features is None and ahead and bgroup > 1
+               and len(batches) > 1 and U.is_cuda)
+    # this rank's first batches are read while the templates are prepared
     reader = tm._BatchReader(bfile, [int(b) for b in batches], ops, device=U.device,
-                             ahead=bool(ops.get("read_ahead", True)))
+                             ahead=ahead, depth=bgroup + 1 if grouped else 1)
     try:
         st, tF = _match_range(ops, bfile, batches, U, device, match, features, prepare,
-                              progress_bar, reader)
+                              progress_bar, reader, bgroup if grouped else 0)
     finally:
         reader.close()
     if distributed:
@@ -120,7 +125,7 @@ def extract_sharded(ops, bfile, U, device=None, dst: int = 0, group=None,
 
 
 def _match_range(ops, bfile, batches, U, device, match, features, prepare, progress_bar,
-                 reader):
+                 reader, group=0):
     if prepare is None:
         def prepare(o, Ut):
             iCC, iCC_mask, iU, Ucc = tm.prepare_extract(
@@ -134,6 +139,12 @@ def _match_range(ops, bfile, batches, U, device, match, features, prepare, progr
         m, f = tm._match_features(ops, W, iCC.to(U.device).contiguous(), iU, Ucc)
         match = match or m
         features = features or f
+    if group:
+        W = ops["wPCA"].contiguous()
+        return tm.extract_grouped(ops, bfile, batches, U, ctc,
+                                  (W, iCC.to(U.device).contiguous(), iU, Ucc), group=group,
+                                  teams=ops.get("batch_teams"), progress_bar=progress_bar,
+                                  reader=reader)
     return tm.extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar,
                               reader=reader)
 

@@ -453,12 +453,14 @@ class _BatchReader:
     that stream may still read it.
     """
 
-    def __init__(self, bfile, order, ops, device=None, ahead=True):
+    def __init__(self, bfile, order, ops, device=None, ahead=True, depth=1):
         self.bfile, self.order, self.ops = bfile, list(order), ops
         self.device = torch.device(device) if device is not None else None
         self.pool = None
         self.stream = None
-        self.next = None
+        self.pending = []               # futures of order[self.submitted - len(pending):]
+        self.submitted = 0
+        self.depth = max(1, int(depth))
         self.filtered = None
         from . import filtered          # imports this module's stream helper
         if self.device is not None and self.device.type == "cuda" \
@@ -466,46 +468,91 @@ class _BatchReader:
             self.filtered = filtered.batches_for(bfile, self.device)
         if ahead and len(self.order) > 1:
             self.pool, self.stream = _reader(self.device or torch.device("cpu"))
-            self.next = self.pool.submit(self._read, self.order[0])
+            self._fill()
+
+    def _fill(self):
+        while len(self.pending) < self.depth and self.submitted < len(self.order):
+            self.pending.append(self.pool.submit(self._read, self.order[self.submitted]))
+            self.submitted += 1
 
     def _load(self, ibatch):
         if self.filtered is None:
             return self.bfile.padded_batch_to_torch(ibatch, self.ops)
-        X = self.filtered.batch(ibatch, self.ops)
-        self.filtered.check()
-        return X
+        return self.filtered.batch(ibatch, self.ops)
 
     def _read(self, ibatch):
+        """(X, event): the event marks the end of X's copy and filter on the
+        reader's stream (None: X is complete)."""
         dev = self.device
         if self.pool is None or dev is None or dev.type != "cuda":
-            return self._load(ibatch)
+            X = self._load(ibatch)
+            if self.filtered is not None:
+                self.filtered.check()
+            return X, None
         s = self.stream
         with torch.cuda.device(dev), torch.cuda.stream(s):
             X = self._load(ibatch)
+            if self.filtered is not None:
+                # the device source is stream-ordered: the consumer waits on
+                # the event, and the host cuts the next window meanwhile
+                ev = torch.cuda.Event()
+                ev.record(s)
+                return X, ev
         s.synchronize()
-        return X
+        return X, None
 
     def get(self, pos):
-        """The batch ``order[pos]``; positions are taken in increasing order."""
+        """The batch ``order[pos]``; positions are taken in increasing order,
+        with up to ``depth`` reads in flight ahead of the consumer."""
         if self.pool is None:
-            return self._read(self.order[pos])
-        X = self.next.result()
-        self.next = (self.pool.submit(self._read, self.order[pos + 1])
-                     if pos + 1 < len(self.order) else None)
+            return self._read(self.order[pos])[0]
+        X, ev = self.pending.pop(0).result()
+        self._fill()
         if isinstance(X, torch.Tensor) and X.is_cuda:
-            X.record_stream(torch.cuda.current_stream(X.device))
+            cur = torch.cuda.current_stream(X.device)
+            if ev is not None:
+                cur.wait_event(ev)
+            X.record_stream(cur)
         return X
 
     def close(self):
         # leave no read of ours running on the shared worker
-        if self.next is not None and not self.next.cancel():
-            try:
-                self.next.result()
-            except Exception:
-                pass
-        self.next = None
+        for f in self.pending:
+            if not f.cancel():
+                try:
+                    f.result()
+                except Exception:
+                    pass
+        self.pending = []
         self.pool = None
         self.filtered = None
+
+    def check(self):
+        """Raise if the device batch source reported an error for any batch
+        read so far (call after the last batch is consumed)."""
+        if self.filtered is not None:
+            self.filtered.check()
+
+
+def _rows_host(ops, bfile, ibatch, st_h, th_h, tf_h):
+    """Host rows ``[N, 3]`` and features of one matched batch, as
+    kilosort/template_matching.py:88-108 forms them: batch 0 drops the spikes
+    whose aligned time would be negative, the time is shifted by the batch's
+    start and aligned to nt0min in float64 (exact for sample indices)."""
+    nt = ops["nt"]
+    if ibatch == 0:
+        keep = ~((st_h[:, 0] - nt - nt // 2 + ops["nt0min"]) < 0)
+        st_h, th_h, tf_h = st_h[keep], th_h[keep], tf_h[keep]
+    t_shift = ibatch * bfile.batch_downsampling * (ops["batch_size"])
+    rows = np.empty((len(st_h), 3), "float64")
+    rows[:, 0] = ((st_h[:, 0].astype("float64") - nt) + t_shift) - nt // 2 + ops["nt0min"]
+    rows[:, 1] = st_h[:, 1]
+    rows[:, 2] = th_h.reshape(-1)
+    return rows, torch.from_numpy(np.ascontiguousarray(tf_h))
+
+
+def _batch_rows(ops, bfile, ibatch, stt, th_amps, xfeat):
+    return _rows_host(ops, bfile, ibatch, *to_host(stt, th_amps, xfeat))
 
 
 def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=None,
@@ -545,23 +592,137 @@ def extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar=N
             X = reader.get(pos)
             stt, amps, th_amps, Xres = match(X, U, ctc, X.device)
             xfeat = features(Xres, stt, amps)
-            if ibatch == 0:
-                neg = (stt[:, 0] - nt - nt // 2 + ops["nt0min"]) < 0
-                stt = stt[~neg, :]
-                xfeat = xfeat[~neg]
-                amps = amps[~neg, :]
-                th_amps = th_amps[~neg, :]
-            t_shift = ibatch * bfile.batch_downsampling * (ops["batch_size"])
-            st_h, th_h, tf_h = to_host(stt, th_amps, xfeat)
-            # float64 as the reference computes them (exact for sample indices)
-            rows = np.empty((len(st_h), 3), "float64")
-            rows[:, 0] = ((st_h[:, 0].astype("float64") - nt) + t_shift) - nt // 2 + ops["nt0min"]
-            rows[:, 1] = st_h[:, 1]
-            rows[:, 2] = th_h.reshape(-1)
+            rows, tf = _batch_rows(ops, bfile, ibatch, stt, th_amps, xfeat)
             sts.append(rows)
-            tFs.append(torch.from_numpy(tf_h))
+            tFs.append(tf)
             if progress_bar is not None:
                 progress_bar.emit(int((ibatch + 1) / bfile.n_batches * 100))
+        reader.check()
+    except Exception:
+        logger.exception(f"Error in kilosort_b200.extract on batch {ibatch}")
+        raise
+    finally:
+        reader.close()
+    st = np.concatenate(sts) if sts else np.zeros((0, 3), "float64")
+    tF = torch.cat(tFs) if tFs else torch.zeros((0, nC, ops["settings"]["n_pcs"]))
+    return st, tF
+
+
+def extract_grouped(ops, bfile, batches, U, ctc, feat, group=4, teams=None,
+                    progress_bar=None, reader=None):
+    """`extract_batches` with the batches matched ``group`` at a time by one
+    ``ks_match_batches`` launch (the batched matcher: each batch's peel
+    equals its own ``run_matching``, bit for bit), so a team of blocks works on
+    every batch of the group at once instead of the whole device on one batch.
+    ``feat`` = (wPCA, iCC, iU, Ucc) on the device.
+
+    Group sizes ramp up as 1, 2, 4, ... to ``group``, so the first launch
+    starts after one batch is read.  The reader keeps a group and one batch in
+    flight ahead of the matcher.
+    Each group's PC features are enqueued right behind its launch with the
+    spike counts read on the device (``ks_features_counted``), so nothing
+    waits for the host between the launches.  Two sets of outputs alternate:
+    while group g is matched, the rows and features of group g-1 are copied to
+    the host on a side stream (copies only, which run beside the peel), and
+    group g+1 is launched once they have arrived.  ``teams`` defaults to one
+    team per batch.  Returns the same rows and features, in batch order, as
+    `extract_batches`.
+    """
+    from . import batched as bt
+    batches = [int(b) for b in batches]
+    dev = U.device
+    nt = int(ops["nt"])
+    proj = ops.get("projection", _default_projection)
+    W, iCC, iU, Ucc = feat
+    nC, K, P = Ucc.shape
+    cap = int(ops.get("spike_capacity", DEFAULT_CAPACITY))
+    rec = bt.Recording(U=U, wPCA=ops["wPCA"], ctc=ctc, Th=ops["Th_learned"], nt=nt,
+                       max_peels=int(ops["max_peels"]), capacity=cap, ctcT=_ctcT.get(ctc, nt))
+    if reader is None:
+        reader = _BatchReader(bfile, batches, ops, device=dev, ahead=True, depth=group + 1)
+    main = torch.cuda.current_stream(dev)
+    aux = torch.cuda.Stream(dev)
+    lib = _lib.load()
+    sts, tFs = [], []
+    slots = [None, None]                  # (outs, info, tF buffers) per parity
+    ws = None
+    prev = None
+    ibatch = -1
+
+    def finish(prev):
+        nonlocal ibatch
+        grp, outs, info, tfs, done, _items = prev
+        with torch.cuda.stream(aux):
+            aux.wait_event(done)
+            host = to_host(info)[0]
+            counts = []
+            for i, ib in enumerate(grp):
+                ibatch = ib
+                n, status, _it, need = (int(v) for v in host[i])
+                if status == _lib.KS_ERR_OVERFLOW:
+                    raise RuntimeError(f"extract: batch {ib} needs {need} spikes, above the "
+                                       f"capacity {cap}; raise ops['spike_capacity']")
+                if status != _lib.KS_OK:
+                    raise _lib.KilosortB200Error(status, f"extract: batch {ib}: device status "
+                                                 f"{status} ({_lib.status_message(status)})")
+                counts.append(n)
+            parts = []
+            for i, n in enumerate(counts):
+                parts += [outs[i].st[:n], outs[i].th_amps[:n], tfs[i][:n]]
+            got = to_host(*parts)
+        for i, ib in enumerate(grp):
+            rows, tf = _rows_host(ops, bfile, ib, *got[3 * i:3 * i + 3])
+            sts.append(rows)
+            tFs.append(tf)
+            if progress_bar is not None:
+                progress_bar.emit(int((ib + 1) / bfile.n_batches * 100))
+
+    # group sizes 1, 2, 4, ... up to `group`: the first launch starts after one
+    # batch is read instead of a whole group
+    sizes, left, g = [], len(batches), 1
+    while left > 0:
+        sizes.append(min(g, group, left))
+        left -= sizes[-1]
+        g *= 2
+    try:
+        pos = 0
+        for gi, size in enumerate(sizes):
+            g0 = pos
+            grp = batches[g0:g0 + size]
+            Xs = [reader.get(pos + i) for i in range(len(grp))]
+            pos += len(grp)
+            items = [(X, 0) for X in Xs]
+            slot = gi % 2
+            if slots[slot] is None or slots[slot][0][0].Xres.shape != Xs[0].shape:
+                # a full group's outputs; smaller groups use the first entries
+                Cn, L = Xs[0].shape
+                slots[slot] = ([bt._Outputs(rec, Cn, L, dev) for _ in range(group)],
+                               torch.empty((group, 4), dtype=torch.int64, device=dev),
+                               [torch.empty((cap, nC, P), dtype=torch.float32, device=dev)
+                                for _ in range(group)])
+            outs, info, tfs = (slots[slot][0][:len(grp)], slots[slot][1][:len(grp)],
+                               slots[slot][2][:len(grp)])
+            t = int(teams) if teams else len(grp)
+            need = bt.workspace_size([rec], items, proj, t)
+            if ws is None or ws.numel() < need:
+                ws = torch.empty(need, dtype=torch.uint8, device=dev)
+            bt._launch([rec], items, outs, info, ws, proj, t)
+            for i, (X, o) in enumerate(zip(Xs, outs)):
+                Cn, L = o.Xres.shape
+                _lib.check(lib.ks_features_counted(
+                    _ptr(o.Xres), _ptr(o.st), _ptr(o.amps), _ptr(W), _ptr(iCC), _ptr(iU),
+                    _ptr(Ucc), Cn, L, K, P, W.shape[1], nC, _ptr(info[i]), cap,
+                    _ptr(tfs[i]), _stream(dev)), "ks_features_counted")
+            done = torch.cuda.Event()
+            done.record(main)
+            if prev is not None:
+                finish(prev)
+            prev = (grp, outs, info, tfs, done, items)
+        if prev is not None:
+            finish(prev)
+            prev = None
+        main.wait_stream(aux)
+        reader.check()
     except Exception:
         logger.exception(f"Error in kilosort_b200.extract on batch {ibatch}")
         raise
@@ -590,9 +751,12 @@ def extract(ops, bfile, U, device=torch.device("cuda"), progress_bar=None):
     nC = ops["settings"]["nearest_chans"]
     position_limit = ops["settings"]["position_limit"]
     batches = np.arange(bfile.n_batches, dtype=np.int64)
-    # the first batch is read (and filtered) while the templates are prepared
+    group = int(ops.get("batch_group", 4))
+    ahead = bool(ops.get("read_ahead", True))
+    grouped = ahead and group > 1 and len(batches) > 1 and U.is_cuda
+    # the first batches are read (and filtered) while the templates are prepared
     reader = _BatchReader(bfile, [int(b) for b in batches], ops, device=U.device,
-                          ahead=bool(ops.get("read_ahead", True)))
+                          ahead=ahead, depth=group + 1 if grouped else 1)
     try:
         iCC, iCC_mask, iU, Ucc = prepare_extract(ops["xc"], ops["yc"], U, nC,
                                                  position_limit, device=device)
@@ -606,8 +770,13 @@ def extract(ops, bfile, U, device=torch.device("cuda"), progress_bar=None):
     except Exception:
         reader.close()
         raise
-    st, tF = extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar,
-                             reader=reader)
+    if grouped:
+        st, tF = extract_grouped(ops, bfile, batches, U, ctc, (W, iCCd, iU, Ucc),
+                                 group=group, teams=ops.get("batch_teams"),
+                                 progress_bar=progress_bar, reader=reader)
+    else:
+        st, tF = extract_batches(ops, bfile, batches, U, ctc, match, features, progress_bar,
+                                 reader=reader)
     st, tF = sort_spikes(st, tF)
     return st, tF, ops
 

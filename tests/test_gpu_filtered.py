@@ -163,3 +163,37 @@ def test_full_size_device_filter_vs_reference_filter(cuda_device, monkeypatch):
     assert len(calls) == 3                                         # the reference filter ran
     a = _compare(st, tF, st_r, tF_r, "full size")
     assert a["n_r"] > 10000
+
+
+def test_grouped_extract_equals_per_batch(cuda_device):
+    """extract matches groups of batches per launch (batched matcher); with
+    ops['batch_group'] = 1 it matches batch by batch.  Same rows and features
+    bit for bit, with a short last group (6 batches in groups of 4) and with
+    groups of 2, in both projections."""
+    rec, raw, ops = _golden_case()
+    U = torch.from_numpy(rec.U).to(DEV)
+    for proj in ("fp32", "bf16x3"):
+        o = dict(ops, projection=proj)
+        st1, tF1, _ = kb.extract(dict(o, batch_group=1), _source(raw), U, device=DEV)
+        for g in (4, 2):
+            st, tF, _ = kb.extract(dict(o, batch_group=g), _source(raw), U, device=DEV)
+            np.testing.assert_array_equal(st, st1)
+            assert torch.equal(tF, tF1)
+
+
+@pytest.mark.parametrize("group", [1, 4])
+def test_filter_error_is_reported_by_extract(cuda_device, group):
+    """A channel-map entry past the file's channels: the device filter flags
+    KS_ERR_ARG (and reads nothing out of bounds); extract raises it once the
+    batches are consumed, per-batch and grouped."""
+    from kilosort_b200 import _lib
+    rec, raw, ops = _golden_case()
+    cmap = np.array(G["chan_map"]).copy()
+    cmap[5] = raw.shape[1]                      # one past the last file channel
+    src = synth.FilteredBinary(raw, NT=int(G["NT"]), nt=61, chan_map=cmap,
+                               hp_filter=highpass_filter(), whiten_mat=torch.from_numpy(G["W"]),
+                               dshift=G["dshift"], device=DEV)
+    with pytest.raises(_lib.KilosortB200Error) as e:
+        kb.extract(dict(ops, batch_group=group), src, torch.from_numpy(rec.U).to(DEV),
+                   device=DEV)
+    assert e.value.status == _lib.KS_ERR_ARG
