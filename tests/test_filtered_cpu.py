@@ -164,3 +164,19 @@ def test_tiled_samples_repeat_the_base_file():
         np.testing.assert_array_equal(t[s:e], full[s:e])
     src = synth.FilteredBinary(t, NT=9, nt=2, device="cpu")
     assert src.n_batches == int(np.ceil(80 / 9))
+
+
+def test_downsampled_batches_match_the_oracle_read(case):
+    """batch_downsampling = 2: batch i reads the file's batch 2i (io.py:791, 788),
+    through filtered.padded_window and through the oracle's restatement of
+    padded_batch_to_torch; the last scaled batch is padded as the reference
+    pads the batch whose scaled index is n_batches - 1."""
+    _, raw = case
+    src = _source(raw, batch_downsampling=2)
+    assert src.n_batches == int(G["n_batches"]) // 2
+    L = src.NT + 2 * src.nt
+    out = np.empty((L, src.n_chan_bin), np.int16)
+    for b in range(src.n_batches):
+        filtered.padded_window(src, b, out)
+        ref = op.padded_batch(src, b, "cpu").numpy()
+        np.testing.assert_array_equal(out.T.astype(np.float32), ref)
