@@ -252,15 +252,16 @@ UNEVEN = ("three recordings (C/K = 96/150, 384/600, 384/1000), 200 padded batche
 def uneven_main(args, dev, rank, world):
     """Batched form: every batch of three recordings through ks_match_batches.
 
-    A step is one pass over all batches: groups of --group batches, each a
-    captured CUDA graph (grouped projection, one cooperative peel launch split
-    into autotuned teams, one residual launch).  The same batches through one
-    run_matching call each are timed beside it.  X resident in HBM.
+    A step is one pass over all batches: groups of --group batches (grouped
+    projection, one cooperative peel launch split into autotuned teams, one
+    residual launch each), all captured in one CUDA graph, so a step is one
+    graph launch.  The same batches through one run_matching call each are
+    timed beside it.  X resident in HBM.
     """
     import kilosort_b200 as kb
     from kilosort_b200 import synth
-    from kilosort_b200.batched import (BatchedMatcher, Recording, autotune_teams,
-                                       workspace_size)
+    from kilosort_b200.batched import (BatchedMatcher, MatcherSequence, Recording,
+                                       autotune_teams, workspace_size)
     recs = synth.uneven_recordings(seed=1003, n_batches_total=200)
     mrecs, items, ops_l = [], [], []
     for i, r in enumerate(recs):
@@ -282,14 +283,15 @@ def uneven_main(args, dev, rank, world):
     ws = torch.empty(max(workspace_size(mrecs, g, "bf16x3", teams) for g in groups),
                      dtype=torch.uint8, device=dev)
     matchers = [BatchedMatcher(mrecs, [(X.shape[1], r) for X, r in g], "bf16x3", teams=teams,
-                               graph=True, workspace=ws) for g in groups]
+                               graph=False, workspace=ws) for g in groups]
     for m, g in zip(matchers, groups):
         for dst, (X, _) in zip(m.X, g):
             dst.copy_(X)
+    # every group of the step in one captured graph (one launch per step)
+    seq = MatcherSequence(matchers)
 
     def batched_step():
-        for m in matchers:
-            m.launch()
+        seq.launch()
 
     def loop_step():
         for X, r in items:
@@ -324,7 +326,7 @@ def uneven_main(args, dev, rank, world):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (split-bf16 projection)", "data": "synthetic",
         "config": {"workload": UNEVEN, "batches": len(items), "group": args.group,
-                   "teams": teams, "graphs": len(matchers),
+                   "teams": teams, "groups": len(matchers), "graphs": 1,
                    "l2": f"inputs larger than L2 ({sum(X.numel() for X, _ in items) * 4 / 1e9:.1f}"
                          " GB of X per step)", "parallelism": f"replicas x{world}"},
         "spikes_per_step": nsp,

@@ -15,6 +15,8 @@ residual launch.  Each batch gets exactly what ``run_matching`` returns for it.
 * ``autotune_teams`` times candidate team counts on the device and caches the
                      fastest per workload signature; ``autotune_schedule``
                      also picks the number of pipelined groups
+* ``MatcherSequence`` several matchers in turn (one shared workspace) captured
+                     in one CUDA graph: a long workload's pass is one launch
 * ``HostPipeline``   batches in host memory: two captured matchers alternate
                      so transfers and read-back overlap the matching
 """
@@ -365,6 +367,49 @@ class BatchedMatcher:
                 dst.copy_(src, non_blocking=True)
         self.launch()
         return self.results()
+
+
+class MatcherSequence:
+    """Several BatchedMatchers run one after another on one stream (for
+    instance the groups of a long uneven workload sharing one workspace),
+    captured in one CUDA graph: a whole pass is one graph launch.
+
+    Each matcher runs once eagerly first (first-use set-up and autotuning stay
+    out of the capture); a matcher whose residual is written in place gets its
+    inputs put back after that run.
+    """
+
+    def __init__(self, matchers: Sequence["BatchedMatcher"]):
+        self.matchers = list(matchers)
+        if not self.matchers:
+            raise ValueError("no matchers")
+        self.device = self.matchers[0].device
+        self._graph = None
+
+    def launch(self):
+        if self._graph is None:
+            for m in self.matchers:
+                saved = [X.clone() for X, o in zip(m.X, m.outs) if o.Xres is X]
+                m.launch_eager()
+                for X, sv in zip((X for X, o in zip(m.X, m.outs) if o.Xres is X), saved):
+                    X.copy_(sv)
+            torch.cuda.synchronize(self.device)
+            g = torch.cuda.CUDAGraph()
+            s = torch.cuda.Stream(self.device)
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(s):
+                g.capture_begin(capture_error_mode="thread_local")
+                try:
+                    for m in self.matchers:
+                        m._enqueue()
+                finally:
+                    g.capture_end()
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            self._graph = g
+        self._graph.replay()
+
+    def results(self):
+        return [r for m in self.matchers for r in m.results()]
 
 
 class HostPipeline:

@@ -167,3 +167,44 @@ def test_host_pipeline_equals_per_batch(cuda_device):
             assert torch.equal(st, st_r.cpu())
             assert torch.equal(amps, amps_r.cpu())
             assert torch.equal(th, th_r.cpu())
+
+
+def test_matcher_sequence_equals_separate_matchers(cuda_device):
+    """Groups captured in one graph (MatcherSequence, one shared workspace)
+    give what each group's own matcher gives."""
+    import numpy as np
+    import torch
+    from kilosort_b200 import synth
+    from kilosort_b200.batched import BatchedMatcher, MatcherSequence, Recording, workspace_size
+    import kilosort_b200 as kb
+    dev = torch.device("cuda:0")
+    recs = synth.uneven_recordings(seed=1003, n_batches_total=6)
+    mrecs, items = [], []
+    for i, r in enumerate(recs):
+        U = torch.from_numpy(r.U).to(dev)
+        ops = dict(Th_learned=8.0, nt=r.nt, max_peels=100, wPCA=torch.from_numpy(r.wPCA).to(dev))
+        mrecs.append(Recording.from_ops(ops, U, kb.prepare_matching(ops, U)))
+        for b in range(r.n_batches):
+            items.append((torch.from_numpy(np.ascontiguousarray(r.batch(b))).to(dev), i))
+    groups = [items[0:3], items[3:6]]
+    ws = torch.empty(max(workspace_size(mrecs, g, "bf16x3", 2) for g in groups),
+                     dtype=torch.uint8, device=dev)
+    seq_m = [BatchedMatcher(mrecs, [(X.shape[1], r) for X, r in g], "bf16x3", teams=2,
+                            graph=False, workspace=ws) for g in groups]
+    ref_m = [BatchedMatcher(mrecs, [(X.shape[1], r) for X, r in g], "bf16x3", teams=2,
+                            graph=True) for g in groups]
+    for ms in (seq_m, ref_m):
+        for m, g in zip(ms, groups):
+            for dst, (X, _) in zip(m.X, g):
+                dst.copy_(X)
+    seq = MatcherSequence(seq_m)
+    seq.launch()
+    seq.launch()                     # the graph replay
+    got = seq.results()
+    want = []
+    for m in ref_m:
+        m.launch()
+        want.extend(m.results())
+    assert len(got) == len(want) == 6
+    for (st, amps, th, _), (st_r, amps_r, th_r, _) in zip(got, want):
+        assert torch.equal(st, st_r) and torch.equal(amps, amps_r) and torch.equal(th, th_r)
