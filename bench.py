@@ -14,6 +14,9 @@ the host->device copy of X and the device->host copy of the spikes inside the
 timed region, through the pipelined front end (batched.HostPipeline: groups
 of KS_BENCH_E2E_GROUP = 5 batches, copies and read-back beside the matching).
 
+The default line also carries shortened runs of the other workloads
+(`extract_sharded`, `uneven`, `stream`; `--no-extra` skips them).
+
     python bench.py --workload uneven     # three recordings, 200 uneven batches
     python bench.py --workload adjoint    # reconstruction loss + adjoint
     python bench.py --workload extract    # drop-in extract over an int16 filtered file
@@ -63,6 +66,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batches", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extra", action="store_true",
+                   help="np1 workload: skip the extra workloads carried in its line "
+                        "(sharded extract, uneven batches, K=2000 stream)")
     p.add_argument("--workload", default="np1",
                    choices=["np1", "uneven", "adjoint", "stream", "detect", "extract", "filter"],
                    help="np1: C=384/K=600, 20 equal batches (default); uneven: three "
@@ -249,7 +255,7 @@ UNEVEN = ("three recordings (C/K = 96/150, 384/600, 384/1000), 200 padded batche
           "max_peels=100, split-BF16 projection")
 
 
-def uneven_main(args, dev, rank, world):
+def uneven_main(args, dev, rank, world, emit=True):
     """Batched form: every batch of three recordings through ks_match_batches.
 
     A step is one pass over all batches: groups of --group batches (grouped
@@ -338,8 +344,9 @@ def uneven_main(args, dev, rank, world):
         # batch; grouped contraction, peel, residual
         "gpu_launches": sum(3 * len(mrecs) + len(m.items) + 3 for m in matchers),
     }
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
+    return line
 
 ADJOINT = ("fixed-assignment reconstruction loss ||X - R||^2 and its adjoint (dU, dwPCA, "
            "damps): C=384, K=600, one 60000-sample batch (+2*61 pad), spikes of the FP32 "
@@ -477,7 +484,7 @@ STREAM = ("long dense recording, shortened: C=384 (NP1-like), K=2000 templates (
           "template-refinement step per group")
 
 
-def stream_main(args, dev, rank, world):
+def stream_main(args, dev, rank, world, emit=True):
     """Config 5 on a shortened recording: host int16 -> results on the host."""
     import kilosort_b200 as kb  # noqa: F401
     from kilosort_b200 import synth
@@ -547,8 +554,9 @@ def stream_main(args, dev, rank, world):
                 "d2h_bytes_per_step": nsp * 20},
         "clocks": sampler.summary(),
     }
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
+    return line
 
 
 FILTER = ("batch filter of one raw int16 batch on the device: 385 file channels (384 mapped), "
@@ -1117,9 +1125,21 @@ def main():
         # batch, grouped contraction, peel, residual
         "gpu_launches": (3 + nb + 3) if head == "bf16x3_batched" else launches_per_batch * nb,
     }
-    # the drop-in extract sharded over the ranks (every rank takes part)
+    # the other workloads, shortened (every rank takes part): the drop-in
+    # extract sharded over the ranks, the uneven multi-recording batches, the
+    # K=2000 stream
     del Xs, Xh
-    line["extract_sharded"] = extract_sharded_block(args, dev, rank, world)
+    if not args.no_extra:
+        line["extract_sharded"] = extract_sharded_block(args, dev, rank, world)
+        short = argparse.Namespace(**dict(vars(args), steps=2, warmup=2, batches=20))
+        keep = ("value", "unit", "ms_per_step", "per_batch_run_matching",
+                "speedup_batched_vs_per_batch", "spikes_per_step", "refinements_per_step",
+                "clocks")
+        for name, fn in (("uneven", uneven_main), ("stream", stream_main)):
+            sub = fn(short, dev, rank, world, emit=False)
+            line[name] = {k: sub[k] for k in keep if k in sub}
+            line[name]["workload"] = sub["config"]["workload"]
+            line[name]["steps"] = short.steps
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
