@@ -415,8 +415,10 @@ class MatcherSequence:
 class HostPipeline:
     """Match batches held in host memory, transfers overlapped with matching.
 
-    The batches are split into consecutive groups of ``group``; two captured
-    ``BatchedMatcher`` graphs alternate, so while group g is matched the
+    The batches are split into consecutive groups whose sizes ramp 1, 2, 4, ...
+    up to ``group`` (the first launch waits for one batch's copy instead of a
+    whole group's); two captured ``BatchedMatcher`` graphs alternate, so while
+    group g is matched the
     copies of group g+1 into the other matcher's inputs (copy stream) and
     the read-back of group g-1's spikes (read-back stream) proceed.  Host
     batches should be page-locked (``pin_memory``) for the copies to be
@@ -434,7 +436,12 @@ class HostPipeline:
         self.group = max(1, int(group))
         self.device = self.recs[0].U.device
         n = len(self.lengths)
-        self.groups = [list(range(g0, min(g0 + self.group, n))) for g0 in range(0, n, self.group)]
+        self.groups, b0, size = [], 0, 1
+        while b0 < n:
+            k = min(size, self.group, n - b0)
+            self.groups.append(list(range(b0, b0 + k)))
+            b0 += k
+            size *= 2
         self._matchers = {}
         self.copy = torch.cuda.Stream(self.device)
         self.readback = torch.cuda.Stream(self.device)
