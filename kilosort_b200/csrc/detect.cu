@@ -244,21 +244,27 @@ ks_detect_scores_tiled_kernel(const float* __restrict__ BT, long long ldb, int n
           for (int k = 0; k < NK; ++k) a[q][k] = fmaf(wq, bk[k], a[q][k]);
         }
       }
-      // largest magnitude, first index in (size, waveform) order
+      // largest magnitude, first index in (size, waveform) order: the
+      // maximum first (NaN never wins, as in a strict > scan), then the first
+      // entry that reaches it
       float best = -1.f, bval = 0.f;
       int bidx = 0;
 #pragma unroll
       for (int q = 0; q < NS; ++q)
 #pragma unroll
         for (int k = 0; k < NK; ++k)
-          if (q < ns && k < nk) {
-            const float m = fabsf(a[q][k]);
-            if (m > best) {
-              best = m;
-              bval = a[q][k];
-              bidx = q * nk + k;
-            }
+          if (q < ns && k < nk) best = fmaxf(best, fabsf(a[q][k]));
+      bool found = false;
+#pragma unroll
+      for (int q = NS - 1; q >= 0; --q)
+#pragma unroll
+        for (int k = NK - 1; k >= 0; --k)
+          if (q < ns && k < nk && fabsf(a[q][k]) == best) {
+            found = true;
+            bval = a[q][k];
+            bidx = q * nk + k;
           }
+      if (!found) best = -1.f;
       if (f < Nfilt && t < L) {
         const int sg = bval > 0.f ? 1 : (bval < 0.f ? -1 : 0);
         As[(long long)f * L + t] = best;
