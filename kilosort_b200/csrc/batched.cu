@@ -147,7 +147,10 @@ __device__ __forceinline__ void peel_multi_body(const MultiParams& p, char* smem
     if (threadIdx.x == 0) fill_args(p, p.order[i], tbase, sa);
     __syncthreads();
     const Smem s = carve_smem(sa, smem_raw, true);
-    const PeelOutcome o = run_peel<kRows, true>(sa, s, rank, (unsigned)p.team_size, epoch);
+    // the lean fold (group_tile<true>): teams work through many tiles per
+    // phase here, so fewer instructions per row pay; the single-batch
+    // launch, bound by its phase barriers, keeps the other form
+    const PeelOutcome o = run_peel<kRows, true, true>(sa, s, rank, (unsigned)p.team_size, epoch);
     if (o.status != KS_OK) {
       if (o.status == KS_ERR_OVERFLOW) continue;   // that batch only
       break;

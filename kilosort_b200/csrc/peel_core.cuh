@@ -649,6 +649,7 @@ __device__ __forceinline__ LaneEntries lane_entries(const TouchList& tl, int c, 
 // smaller template index); rows with sq = 0 and a normal nm have the
 // quotient +0 exactly, and rows whose approx is NaN or tiny are folded
 // exactly too.
+template <bool kLazy>
 __device__ unsigned long long group_tile(const PeelArgs& a, const Smem& s, const TouchList& tl,
                                          int blk, int g, bool nd, const LaneEntries& le,
                                          bool store, int jl, float2 nl, int lane, int warp) {
@@ -709,6 +710,10 @@ __device__ unsigned long long group_tile(const PeelArgs& a, const Smem& s, const
       }
     }
   }
+  float best = -1.f;
+  int arg = 0x7fffffff;
+  int emin = 255;                             // smallest exponent field over the rows
+  if constexpr (!kLazy) {
   // pass 1, branch-free over all kGroup rows (rows past nrow and columns
   // without nd only compute, their results unused): the (single peak)
   // subtraction, the write-back, the smallest exponent, and for the best
@@ -720,7 +725,7 @@ __device__ unsigned long long group_tile(const PeelArgs& a, const Smem& s, const
   const bool sub = fused && le.e0 >= 0;
   constexpr float kTiny = 7.8886091e-31f;     // 2^-100
   float m = -1.f, m2 = -1.f;
-  int rm = -1, jz = 0x7fffffff, emin = 255;
+  int rm = -1, jz = 0x7fffffff;
   unsigned spec = 0u;
 #pragma unroll 8
   for (int r = 0; r < kGroup; ++r) {
@@ -751,8 +756,6 @@ __device__ unsigned long long group_tile(const PeelArgs& a, const Smem& s, const
   const bool regime_a = m >= 8.0779356e-28f;  // 2^-90
   const float thr = regime_a ? m * 0.99999905f : kTiny;
   const bool scan = !regime_a || m2 >= thr;
-  float best = -1.f;
-  int arg = 0x7fffffff;
   if (jz != 0x7fffffff) {
     best = 0.f;
     arg = jz;
@@ -789,6 +792,100 @@ __device__ unsigned long long group_tile(const PeelArgs& a, const Smem& s, const
       arg = j;
     }
   }
+  } else {
+  // pass 1 over the group's rows, branch-free in the columns (a column
+  // without nd computes too, its results unused): the (single peak)
+  // subtraction, the write-back, the smallest exponent, and for the best
+  // score the largest approx m with its first row rm and the largest approx
+  // m2 of the other rows.  Rows with an approx below 2^-100 take part in m
+  // and m2 without changing what follows (the candidate level is at least
+  // 2^-90 when m is, and below it every row >= 2^-100 is a candidate), NaN
+  // approx never does.  Rows that need an exact quotient whatever m is
+  // (approx NaN, or below 2^-100 with sq > 0) only raise a flag here and are
+  // found by a second pass when some column has one.
+  float* bdst = a.Bt + (size_t)blk * K * kCol + lane;
+  const bool sub = fused && le.e0 >= 0;
+  constexpr float kTiny = 7.8886091e-31f;     // 2^-100
+  float m = -1.f, m2 = -1.f;
+  int rm = -1;
+  bool anyspec = false;
+#pragma unroll 8
+  for (int r = 0; r < nrow; ++r) {
+    const int j = __shfl_sync(0xffffffffu, jl, r);
+    const float nmy = __shfl_sync(0xffffffffu, nl.y, r);
+    const float b0 = Bs[r * 32 + lane];
+    const float b1 = __fsub_rn(b0, __fmul_rn(amp0, Cs[r * 32 + lane]));
+    const float b = sub ? b1 : b0;
+    if (nd && store) bdst[(size_t)j * kCol] = b;
+    emin = min(emin, noop_expo(b));
+    const float rl = b > 0.f ? b : 0.f;
+    const float sq = __fmul_rn(rl, rl);
+    const float ap = __fmul_rn(sq, nmy);
+    const bool top = ap > m;
+    m2 = top ? m : fmaxf(m2, ap);
+    rm = top ? r : rm;
+    m = top ? ap : m;
+    anyspec |= (ap != ap) || (ap < kTiny && sq != 0.f);
+  }
+  // Candidates for the best: with m >= 2^-90 the rows whose approx is at
+  // least (1 - 2^-20) m -- only rm, unless m2 reaches that level; below
+  // 2^-90 every row with approx >= 2^-100.  Rows with a smaller approx
+  // cannot reach the exact quotient of rm (or 2^-100 and the zeros), so the
+  // result is that of folding every row.
+  const bool regime_a = m >= 8.0779356e-28f;  // 2^-90
+  const float thr = regime_a ? m * 0.99999905f : kTiny;
+  const bool scan = !regime_a || m2 >= thr;
+  unsigned cand = 0u;
+  if (regime_a && !scan) cand |= 1u << rm;
+  if (__any_sync(0xffffffffu, nd && (scan || anyspec))) {
+#pragma unroll 8
+    for (int r = 0; r < nrow; ++r) {
+      const float nmy = __shfl_sync(0xffffffffu, nl.y, r);
+      const float b0 = Bs[r * 32 + lane];
+      const float b1 = __fsub_rn(b0, __fmul_rn(amp0, Cs[r * 32 + lane]));
+      const float b = sub ? b1 : b0;
+      const float rl = b > 0.f ? b : 0.f;
+      const float sq = __fmul_rn(rl, rl);
+      const float ap = __fmul_rn(sq, nmy);
+      const bool sp = ap != ap || (ap < kTiny && sq != 0.f);
+      cand |= ((scan && ap >= thr) || sp) ? (1u << r) : 0u;
+    }
+  }
+  // exact quotients of the candidates (usually only rm, converged)
+  if (!nd) cand = 0u;
+  for (unsigned mm = cand; mm; mm &= mm - 1u) {
+    const int r = __ffs(mm) - 1;
+    float b = Bs[r * 32 + lane];
+    if (sub) b = __fsub_rn(b, __fmul_rn(amp0, Cs[r * 32 + lane]));
+    const float2 jn = rtab[r];
+    const int j = __float_as_int(jn.x);
+    const float rl = b > 0.f ? b : 0.f;
+    const float sq = __fmul_rn(rl, rl);
+    const bool normal = jn.y >= 1.17549435e-38f && jn.y <= 3.40282347e38f;
+    const float cf = (sq == 0.f && normal) ? 0.f : __fdiv_rn(sq, jn.y);
+    if (cf > best || (cf == best && j < arg)) {
+      best = cf;
+      arg = j;
+    }
+  }
+  // rows whose score is exactly 0 (sq = 0 and 1/nm not NaN) can only matter
+  // when no candidate scored above 0: fold them then (score 0, smaller
+  // template index first)
+  if (__any_sync(0xffffffffu, nd && !(best > 0.f))) {
+    for (int r = 0; r < nrow; ++r) {
+      const int j = __shfl_sync(0xffffffffu, jl, r);
+      const float nmy = __shfl_sync(0xffffffffu, nl.y, r);
+      float b = Bs[r * 32 + lane];
+      if (sub) b = __fsub_rn(b, __fmul_rn(amp0, Cs[r * 32 + lane]));
+      const float rl = b > 0.f ? b : 0.f;
+      const float sq = __fmul_rn(rl, rl);
+      if (nd && sq == 0.f && nmy == nmy && (0.f > best || (0.f == best && j < arg))) {
+        best = 0.f;
+        arg = j;
+      }
+    }
+  }
+  }
   unsigned long long gb = 0ull;
   if (nd) {
     gb = best >= 0.f ? pack_score(best, arg) : 0ull;
@@ -812,6 +909,7 @@ __device__ __forceinline__ void group_rows(const PeelArgs& a, int g, int lane, i
 
 // Initial scores of groups [g_lo, g_hi) of block blk (nothing subtracted):
 // every group's gbest and gexp, and the column maxima folded into pack_out.
+template <bool kLazy>
 __device__ void group_init_item(const PeelArgs& a, const Smem& s, int blk, int g_lo, int g_hi,
                                 unsigned long long* pack_out, int lane, int warp) {
   const int c = blk * kCol + lane;
@@ -823,7 +921,8 @@ __device__ void group_init_item(const PeelArgs& a, const Smem& s, int blk, int g
     int jl;
     float2 nl;
     group_rows(a, g, lane, jl, nl);
-    const unsigned long long gb = group_tile(a, s, none, blk, g, colok, le, false, jl, nl, lane, warp);
+    const unsigned long long gb =
+        group_tile<kLazy>(a, s, none, blk, g, colok, le, false, jl, nl, lane, warp);
     colbest = gb > colbest ? gb : colbest;
   }
   if (colok && colbest) atomicMax(&pack_out[c], colbest);
@@ -937,6 +1036,7 @@ __device__ __forceinline__ UnitFetch unit_fetch(const PeelArgs& a, uint2 u, int 
   return f;
 }
 
+template <bool kLazy>
 __device__ void unit_run(const PeelArgs& a, const Smem& s, const UnitFetch& f,
                          unsigned long long* pack_out, int lane, int warp) {
   const int blk = (int)(f.u.x >> 11), g = (int)(f.u.x & 2047u);
@@ -958,7 +1058,8 @@ __device__ void unit_run(const PeelArgs& a, const Smem& s, const UnitFetch& f,
   const TouchList tl{n, tau, kk, amp};
   const int c = blk * kCol + lane;
   const LaneEntries le = lane_entries(tl, c, c < a.L, a.nt);
-  const unsigned long long gb = group_tile(a, s, tl, blk, g, nd, le, true, f.jl, f.nl, lane, warp);
+  const unsigned long long gb =
+      group_tile<kLazy>(a, s, tl, blk, g, nd, le, true, f.jl, f.nl, lane, warp);
   if (nd && gb) atomicMax(&pack_out[c], gb);
 }
 
@@ -990,7 +1091,7 @@ struct PeelOutcome {
 // (written by one thread) and is returned to every thread.  When the status
 // is KS_OK every record and residual list of the batch is complete and
 // visible to the team (the last pass ended at a team barrier).
-template <int kRows, bool kGrouped>
+template <int kRows, bool kGrouped, bool kLazy = false>
 __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsigned G,
                                 unsigned& epoch) {
   const int tid = threadIdx.x;
@@ -1034,7 +1135,7 @@ __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsi
       const long long n_items = (long long)a.nblk * rg;
       for (long long w = gwarp; w < n_items; w += nwarps) {
         const int blk = (int)(w / rg), r = (int)(w % rg);
-        group_init_item(a, s, blk, r * kInitGroups, min(a.ng, (r + 1) * kInitGroups), pinit,
+        group_init_item<kLazy>(a, s, blk, r * kInitGroups, min(a.ng, (r + 1) * kInitGroups), pinit,
                         lane, warp);
       }
     } else {
@@ -1132,7 +1233,7 @@ __device__ PeelOutcome run_peel(const PeelArgs& a, const Smem& s, int rank, unsi
             nxt = unit_fetch(a, make_uint2(__shfl_sync(0xffffffffu, rec.x, i + 1),
                                            __shfl_sync(0xffffffffu, rec.y, i + 1)),
                              lane);
-          unit_run(a, s, cur, pcur, lane, warp);
+          unit_run<kLazy>(a, s, cur, pcur, lane, warp);
           cur = nxt;
         }
       }
