@@ -649,6 +649,9 @@ __device__ __forceinline__ LaneEntries lane_entries(const TouchList& tl, int c, 
 // smaller template index); rows with sq = 0 and a normal nm have the
 // quotient +0 exactly, and rows whose approx is NaN or tiny are folded
 // exactly too.
+// kLazy selects the lean form of that fold (the batched launch): the same
+// result with fewer instructions per row, the rare cases (zero scores, NaN or
+// tiny approximations) found by second passes that run only when needed.
 template <bool kLazy>
 __device__ unsigned long long group_tile(const PeelArgs& a, const Smem& s, const TouchList& tl,
                                          int blk, int g, bool nd, const LaneEntries& le,
