@@ -112,7 +112,7 @@ __device__ void fill_args(const MultiParams& p, int b, char* team, PeelArgs& a) 
 // ks_residual_kernel does), so one team's residual work fills the barrier
 // waits of the others.  A team stops at its first error (info of its later
 // batches keeps the "not run" value).
-template <int kRows>
+template <int kRows, bool kLean>
 __device__ __forceinline__ void peel_multi_body(const MultiParams& p, char* smem_raw,
                                                 PeelArgs& sa);
 
@@ -120,7 +120,20 @@ __device__ __forceinline__ void peel_multi_body(const MultiParams& p, char* smem
 __global__ void __launch_bounds__(kThreads, 2) peel_multi_kernel(const __grid_constant__ MultiParams p) {
   extern __shared__ __align__(16) char smem_raw[];
   __shared__ PeelArgs sa;
-  peel_multi_body<kRowsPerWarp>(p, smem_raw, sa);
+  peel_multi_body<kRowsPerWarp, false>(p, smem_raw, sa);
+}
+
+// The same with the lean group fold (group_tile<true>), for small teams: a
+// team of at most kLeanTeamBlocks blocks works through tens of tiles per warp
+// and phase, where fewer instructions per row pay; larger teams (few tiles
+// per warp, phases bound by their barriers) measured faster with the other
+// fold.  Results are identical.
+constexpr int kLeanTeamBlocks = 16;
+__global__ void __launch_bounds__(kThreads, 2)
+peel_multi_kernel_lean(const __grid_constant__ MultiParams p) {
+  extern __shared__ __align__(16) char smem_raw[];
+  __shared__ PeelArgs sa;
+  peel_multi_body<kRowsPerWarp, true>(p, smem_raw, sa);
 }
 
 // Beside the projection kernels of the next group: 1 block per SM capped at
@@ -130,10 +143,10 @@ __global__ void __launch_bounds__(kThreads, 2) peel_multi_kernel(const __grid_co
 __global__ void __maxnreg__(80) peel_multi_kernel_shared(const __grid_constant__ MultiParams p) {
   extern __shared__ __align__(16) char smem_raw[];
   __shared__ PeelArgs sa;
-  peel_multi_body<kRowsPerWarp>(p, smem_raw, sa);
+  peel_multi_body<kRowsPerWarp, false>(p, smem_raw, sa);
 }
 
-template <int kRows>
+template <int kRows, bool kLean>
 __device__ __forceinline__ void peel_multi_body(const MultiParams& p, char* smem_raw,
                                                 PeelArgs& sa) {
   const int team = blockIdx.x / p.team_size;
@@ -147,10 +160,7 @@ __device__ __forceinline__ void peel_multi_body(const MultiParams& p, char* smem
     if (threadIdx.x == 0) fill_args(p, p.order[i], tbase, sa);
     __syncthreads();
     const Smem s = carve_smem(sa, smem_raw, true);
-    // the lean fold (group_tile<true>): teams work through many tiles per
-    // phase here, so fewer instructions per row pay; the single-batch
-    // launch, bound by its phase barriers, keeps the other form
-    const PeelOutcome o = run_peel<kRows, true, true>(sa, s, rank, (unsigned)p.team_size, epoch);
+    const PeelOutcome o = run_peel<kRows, true, kLean>(sa, s, rank, (unsigned)p.team_size, epoch);
     if (o.status != KS_OK) {
       if (o.status == KS_ERR_OVERFLOW) continue;   // that batch only
       break;
@@ -524,7 +534,18 @@ extern "C" KS_API int ks_match_batches(const ks_rec_desc* recs, int64_t n_recs,
     cfg.stream = s;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    KS_CUDA(cudaLaunchKernelEx(&cfg, pv.kernel, mp));
+    void (*kernel)(MultiParams) = pv.kernel;
+    if (pv.kernel == peel_multi_kernel && mp.team_size <= kLeanTeamBlocks) {
+      // small teams: the lean fold, if it is as resident as the other form
+      KS_CUDA(cudaFuncSetAttribute(peel_multi_kernel_lean,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      int occ_lean = 0;
+      KS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_lean, peel_multi_kernel_lean,
+                                                            kThreads, smem));
+      if (dev.sm_count * std::min(occ_lean, pv.blocks_per_sm) >= max_blocks)
+        kernel = peel_multi_kernel_lean;
+    }
+    KS_CUDA(cudaLaunchKernelEx(&cfg, kernel, mp));
   }
   // the residual passes ran inside the peel launches
   trace_mark(3, s);
