@@ -237,7 +237,8 @@ class FilteredBatches:
 
     def check(self) -> None:
         """Raise if any batch filtered since the last check reported an error
-        (synchronises with the last one)."""
+        (synchronises with the last one).  Call it when no batch is being
+        filtered on another stream: the status word is cleared here."""
         status = int(to_host(self.sticky)[0][0])
         self.sticky.zero_()
         if status != _lib.KS_OK:
