@@ -180,3 +180,35 @@ def test_downsampled_batches_match_the_oracle_read(case):
         filtered.padded_window(src, b, out)
         ref = op.padded_batch(src, b, "cpu").numpy()
         np.testing.assert_array_equal(out.T.astype(np.float32), ref)
+
+
+class _CountingSource:
+    """A batch source that records the order of its reads."""
+
+    def __init__(self, n):
+        self.n_batches, self.batch_downsampling = n, 1
+        self.reads = []
+
+    def padded_batch_to_torch(self, ibatch, ops=None):
+        self.reads.append(int(ibatch))
+        return torch.full((2, 5), float(ibatch))
+
+
+@pytest.mark.parametrize("depth", [1, 3, 8])
+def test_batch_reader_reads_ahead_in_order(depth):
+    """The extract loop's reader hands over the batches in order with up to
+    `depth` reads in flight, reads each batch once, and close() leaves no read
+    running (a partly consumed reader included)."""
+    from kilosort_b200 import template_matching as tm
+    src = _CountingSource(7)
+    order = [0, 1, 2, 3, 4, 5, 6]
+    r = tm._BatchReader(src, order, {}, device=None, ahead=True, depth=depth)
+    got = [int(r.get(p)[0, 0]) for p in range(len(order))]
+    r.close()
+    assert got == order and src.reads == order
+    src2 = _CountingSource(7)
+    r2 = tm._BatchReader(src2, order, {}, device=None, ahead=True, depth=depth)
+    assert int(r2.get(0)[0, 0]) == 0
+    r2.close()
+    assert not r2.pending and src2.reads == sorted(src2.reads)
+    assert len(src2.reads) <= 1 + depth
