@@ -835,7 +835,7 @@ def main():
     ctc = kb.prepare_matching(ops, U)
     torch.cuda.synchronize()
 
-    # projection forms available in this build
+    # projection forms the built library offers
     forms = ["fp32"]
     try:
         kb.run_matching(dict(ops, projection="bf16x3"), Xs[0], U, ctc, device=dev)

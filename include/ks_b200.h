@@ -41,7 +41,7 @@ extern "C" {
 #define KS_ERR_OVERFLOW 3     /* more spikes than the output capacity */
 #define KS_ERR_TIMEOUT 4      /* a bounded device-side wait ran out */
 #define KS_ERR_WORKSPACE 5    /* workspace smaller than *_workspace_size() */
-#define KS_ERR_UNSUPPORTED 6  /* device or shape not supported by this build */
+#define KS_ERR_UNSUPPORTED 6  /* device or shape not supported by this library */
 #define KS_ERR_DEGENERATE 7   /* exact score plateaus beyond the tie buffer */
 
 /* layout of the score matrix B */

@@ -268,7 +268,7 @@ ks_temporal_tc_kernel(const float* __restrict__ X, const float* __restrict__ W, 
           mma_commit(full0 + 8 * b);
         }
       }
-      // the issuing lane's verdict reaches every producer before the next tile
+      // the issuing lane's decision reaches every producer before the next tile
       if (!group_all(ok, 2, 128)) { ok = false; break; }
     }
     if (pt == 0) {

@@ -13,7 +13,7 @@ the peak test, the amplitudes, y positions and PC features -- is one call of
 The universal waveforms and basis come, as in the reference's ``run``
 (:205-216), either from its built-in templates file (``get_waves``, read from
 the same place the reference keeps its download, $KILOSORT_LOCAL_DOWNLOADS_PATH
-or ~/.kilosort; this build does not download it) or, with
+or ~/.kilosort; this library does not download it) or, with
 ``settings['templates_from_data']``, from the data (``extract_wPCA_wTEMP``,
 :50-92): the isolated single-channel peaks of every 25th batch
 (``ks_snippets``), the exact truncated-SVD basis of their unit-norm snippets
@@ -100,7 +100,7 @@ def template_path(basename="wTEMP.npz"):
 
 def get_waves(ops, device=torch.device("cuda")):
     """kilosort/spikedetect.py:94-98: (wPCA, wTEMP) of the built-in templates
-    file.  The reference downloads the file when it is missing; this build
+    file.  The reference downloads the file when it is missing; this library
     has no download and raises FileNotFoundError instead."""
     path = template_path()
     if not os.path.exists(path):
