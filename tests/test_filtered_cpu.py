@@ -212,3 +212,25 @@ def test_batch_reader_reads_ahead_in_order(depth):
     r2.close()
     assert not r2.pending and src2.reads == sorted(src2.reads)
     assert len(src2.reads) <= 1 + depth
+
+
+def test_device_source_signature_follows_the_settings():
+    """extract keeps a file's device source while the settings it was built
+    from are unchanged: the same object gives the same signature; a new
+    channel map, an in-place change of the whitening matrix, or other flags
+    give a new one."""
+    raw = np.zeros((7000, 6), np.int16)
+    W = torch.eye(4)
+    src = synth.FilteredBinary(raw, NT=3000, chan_map=np.arange(4), whiten_mat=W)
+    sig = filtered._signature(src)
+    assert filtered._signature(src) == sig
+    src.chan_map = np.arange(4)                   # equal values: the same source
+    assert filtered._signature(src) == sig
+    src.chan_map = np.array([0, 1, 2, 5])
+    assert filtered._signature(src) != sig
+    src.chan_map = np.arange(4)
+    W.mul_(2.0)                                    # the same tensor, changed in place
+    assert filtered._signature(src) != sig
+    sig2 = filtered._signature(src)
+    src.do_CAR = False
+    assert filtered._signature(src) != sig2
