@@ -41,3 +41,23 @@ def test_reference_arm_line():
 
 def test_reference_arm_other_ranks_print_nothing():
     assert _run({"RANK": "1", "WORLD_SIZE": "2"}) == []
+
+
+def test_workload_options_parse():
+    """Every workload and the extra-workload switch are accepted by the
+    command line (the device runs need a GPU; the parser does not)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    argv = sys.argv
+    try:
+        for w in ("np1", "uneven", "adjoint", "stream", "detect", "extract", "filter"):
+            sys.argv = ["bench.py", "--workload", w, "--no-extra", "--steps", "2", "--warmup", "3"]
+            a = bench.parse()
+            assert a.workload == w and a.no_extra and a.steps == 2 and a.warmup == 3
+        sys.argv = ["bench.py"]
+        a = bench.parse()
+        assert a.workload == "np1" and not a.no_extra and a.gpus == 1
+    finally:
+        sys.argv = argv
